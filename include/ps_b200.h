@@ -1,0 +1,174 @@
+/*
+ * ps_b200.h -- C ABI of the B200 PeriodSearch fit engine.
+ *
+ * Drop-in replacement for the reference's GPU boundary (start_CUDA.h:2-16 of
+ * PeriodSearch): CUDAPrepare / CUDAPrecalc / CUDAStart / CUDAUnprepare.  The
+ * reference reads part of its input from process globals (globals.h:6-22:
+ * l_curves, l_points, in_rel, weight, normal, d_area, d_sphere, n_coef); here
+ * those travel explicitly in ps_curves / ps_shape.  Nothing in this ABI exits
+ * the process: every entry point returns a ps_status and ps_last_error()
+ * describes the most recent failure.
+ *
+ * Array conventions (all arrays 0-based, owned by the caller, only read):
+ *   ndata        number of real data points (the reference's ndata without
+ *                the 3 convexity pseudo-points it appends)
+ *   tim[i]       JD - jd0 of point i, days
+ *   ee[3*i+k]    unit vector to the observer, ee0[3*i+k] to the Sun
+ *   brightness[i], sig[i] (per-curve mean brightness), sigr2[i] = 1/sig^2,
+ *   weight[i]    per-point weight
+ *   ia[p]        1-based fitted mask, p = 1..ma (ma = n_coef + 8), ia[0] unused
+ *   ia_par[k]    k = 0..2: fitted flags of the three phase-function parameters
+ *   cg_first[k]  k = 0..n_coef-1: initial shape coefficients (ellfit output)
+ *   d_sphere[f*n_coef + k]  Laplace basis value of coefficient k at facet f
+ *   normal[3*f+k], d_area[f]  facet normals and areas of the Gaussian image
+ */
+#ifndef PS_B200_H
+#define PS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ps_status {
+    PS_OK = 0,
+    PS_ERR_ARG = 1,          /* invalid argument or size beyond a limit */
+    PS_ERR_CUDA = 2,         /* CUDA runtime error (message in ps_last_error) */
+    PS_ERR_NOT_PREPARED = 3, /* call ps_gpu_prepare first */
+    PS_ERR_CANCELLED = 4,    /* progress callback asked to stop */
+    PS_ERR_ALLOC = 5         /* device or host allocation failed */
+} ps_status;
+
+#define PS_N_POLES 10
+#define PS_MAX_PAR 96        /* ma <= 89 (lmax <= 8) */
+#define PS_MAX_FAC 1024
+
+/* Device-status bits accumulated over calls (ps_gpu_status). */
+#define PS_DEVSTAT_SINGULAR 1   /* a Gauss-Jordan pivot was exactly zero */
+#define PS_DEVSTAT_NAN_CHISQ 2  /* an evaluation produced NaN chi^2 */
+
+/* Quirk bits (ps_gpu_set_quirks): reproduce documented reference behaviour. */
+#define PS_QUIRK_PRECALC_CONW 1 /* start_CUDA.cu:476 uploads the pointer bits of
+                                   conw_r in CUDAPrecalc: the precalc rms then
+                                   ignores the regularisation term */
+
+typedef struct ps_gpu ps_gpu;
+
+/* The lightcurve layout (globals l_curves, l_points, in_rel). */
+typedef struct ps_curves {
+    int32_t n_curves;            /* real curves, the pseudo-curve excluded */
+    const int32_t *curve_len;    /* [n_curves] points per curve */
+    const int32_t *curve_rel;    /* [n_curves] 1 = relative, 0 = calibrated */
+} ps_curves;
+
+/* The Gaussian-image shape model (globals normal, d_area, d_sphere). */
+typedef struct ps_shape {
+    int32_t n_coef;
+    const double *normal;        /* [numfac*3] */
+    const double *d_area;        /* [numfac] */
+    const double *d_sphere;      /* [numfac*n_coef] */
+} ps_shape;
+
+/* One line of period_search_out (start_CUDA.cu:1200-1229). */
+typedef struct ps_line {
+    double period_h;     /* 24 * per_best */
+    double rms;          /* dev_best */
+    double chisq;        /* rms^2 * ndata */
+    double dark;         /* dark-facet %, or conw_r*escl^2 on the scan's first line */
+    double lambda_deg;   /* [0, 360) */
+    double beta_deg;
+} ps_line;
+
+/* Result of one (frequency, pole) fit. */
+typedef struct ps_fit_result {
+    double dev, dark, per, lambda_deg, beta_deg, chisq;
+    int32_t niter, status;
+} ps_fit_result;
+
+/* Progress callback: frequencies finished / total.  Non-zero return cancels. */
+typedef int (*ps_progress_fn)(void *user, int32_t n_done, int32_t n_total);
+
+/* Replaces CUDAPrepare (start_CUDA.h:2-4, start_CUDA.cu:207-364): opens the
+   device, stores the per-point geometry and the fit constants.  cl is the
+   linear Lambert coefficient (the reference uploads log(cl)). */
+ps_status ps_gpu_prepare(int32_t device, const double *beta_pole, const double *lambda_pole,
+                         const double *par, double cl, double alamda_start, double alamda_incr,
+                         double alamda_incrr, const double *ee, const double *ee0,
+                         const double *tim, double phi0, int32_t ndata, const double *weight,
+                         ps_gpu **handle);
+
+/* Replaces CUDAPrecalc (start_CUDA.h:10-12, start_CUDA.cu:400-789): fits the
+   first 10 trial periods x 10 poles and doubles *conw_r while the mean dark
+   facet is >= 1 %, setting *new_conw = 1 once it is below. */
+ps_status ps_gpu_precalc(ps_gpu *h, double freq_start, double freq_end, double freq_step,
+                         double stop_condition, int32_t n_iter_min, double *conw_r,
+                         int32_t ndata, const int32_t *ia, const int32_t *ia_par,
+                         int32_t *new_conw, const double *cg_first, const double *sig,
+                         const double *sigr2, int32_t numfac, const double *brightness,
+                         const ps_curves *curves, const ps_shape *shape);
+
+/* Replaces CUDAStart (start_CUDA.h:6-8, start_CUDA.cu:792-1245): the full
+   period scan n = n_start_from..n_max.  Instead of printing into an MFILE it
+   fills lines[0..*n_lines) (one per frequency, the best of the 10 poles). */
+ps_status ps_gpu_start(ps_gpu *h, int32_t n_start_from, double freq_start, double freq_end,
+                       double freq_step, double stop_condition, int32_t n_iter_min,
+                       double conw_r, int32_t ndata, const int32_t *ia, const int32_t *ia_par,
+                       const double *cg_first, double escl, const double *sig,
+                       const double *sigr2, int32_t numfac, const double *brightness,
+                       const ps_curves *curves, const ps_shape *shape, ps_line *lines,
+                       int32_t max_lines, int32_t *n_lines, ps_progress_fn progress,
+                       void *user);
+
+/* Replaces CUDAUnprepare (start_CUDA.h:16, start_CUDA.cu:368-385). */
+void ps_gpu_unprepare(ps_gpu *h);
+
+/* ---- finer-grained entry points (no reference counterpart: the reference
+        keeps these steps inside CUDAStart) ---- */
+
+/* Uploads the object and scan configuration used by ps_gpu_fit_items and
+   ps_gpu_eval.  conw_r_rms is the weight used in the rms (normally conw_r). */
+ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_step, double stop_condition,
+                           int32_t n_iter_min, double conw_r, double conw_r_rms, int32_t ndata,
+                           const int32_t *ia, const int32_t *ia_par, const double *cg_first,
+                           const double *sig, const double *sigr2, int32_t numfac,
+                           const double *brightness, const ps_curves *curves,
+                           const ps_shape *shape);
+
+/* Runs n LM fits (frequency index n_freq[i] >= 1, pole index pole[i] in 0..9)
+   with the configured object; results to out[i]. */
+ps_status ps_gpu_fit_items(ps_gpu *h, int32_t n, const int32_t *n_freq, const int32_t *pole,
+                           ps_fit_result *out);
+
+/* As ps_gpu_fit_items, but items and results stay in device memory (pointers
+   from cudaMalloc) and nothing is synchronised: the call only enqueues the
+   fit kernel on the handle's stream.  Used for device-resident timing. */
+ps_status ps_gpu_fit_items_device(ps_gpu *h, int32_t n, const int32_t *d_items,
+                                  ps_fit_result *d_out);
+
+/* One function evaluation (the reference's mrqcof) at the 1-based parameter
+   vector a[0..ma]: chi^2, alpha (mfit x mfit row-major) and beta (mfit). */
+ps_status ps_gpu_eval(ps_gpu *h, const double *a, double *chisq, double *alpha, double *beta,
+                      double *area_sum);
+
+/* Device-status bits (PS_DEVSTAT_*) accumulated since prepare. */
+ps_status ps_gpu_status(ps_gpu *h, int32_t *flags);
+ps_status ps_gpu_set_quirks(ps_gpu *h, int32_t quirks);
+/* The CUDA stream all work of the handle runs on (a cudaStream_t). */
+void *ps_gpu_stream(ps_gpu *h);
+/* Fit CTAs resident per SM and SM count for the configured object. */
+ps_status ps_gpu_occupancy(ps_gpu *h, int32_t *ctas_per_sm, int32_t *n_sm);
+
+/* Host shape setup (trifac.c, areanorm.c, sphfunc.c, ellfit.c of the
+   reference): facet normals, areas, Laplace basis and the ellipsoid fit. */
+ps_status ps_setup_shape(int32_t l_max, int32_t m_max, int32_t nrows, double a, double b, double c,
+                         double *normal, double *d_area, double *d_sphere, double *cg_first);
+int32_t ps_n_coef(int32_t l_max, int32_t m_max);
+
+const char *ps_last_error(void);
+const char *ps_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,93 @@
+// engine.cu -- template dispatch and launch wrappers of the fit kernel.
+#include <cuda_runtime.h>
+
+#include "engine.h"
+#include "fit_kernel.cuh"
+
+namespace psb {
+
+using KernelFn = void (*)(DevObject, DevParams, const FitItem *, int, int *, FitOut *, double *, size_t,
+                          int *, EvalOut, int);
+
+// The shape-derivative accumulators live in registers, so the kernel is
+// compiled per padded coefficient count.
+#define PSB_NCP_LIST(X) X(16) X(24) X(32) X(40) X(48) X(56) X(64) X(72) X(80) X(88)
+
+int padded_ncoef(int n_coef)
+{
+#define PSB_PICK(N) if (n_coef <= N) return N;
+    PSB_NCP_LIST(PSB_PICK)
+#undef PSB_PICK
+    return -1;
+}
+
+size_t fit_smem_bytes(int n_fac, int mfit) { return carve_bytes(n_fac, mfit, nullptr, nullptr); }
+
+size_t fit_scratch_doubles(const DevObject &o)
+{
+    size_t n = (size_t)o.n_points * o.row_stride + (size_t)o.n_curves * (o.ma + 3);
+    return (n + 31) & ~size_t(31);
+}
+
+// One translation unit per instance (fit_inst.cu) exports its kernel.
+#define PSB_DECL(N) KernelFn fit_kernel_ptr_##N();
+PSB_NCP_LIST(PSB_DECL)
+#undef PSB_DECL
+
+static KernelFn kernel_for(int ncp)
+{
+    switch (ncp) {
+#define PSB_CASE(N) \
+    case N:         \
+        return fit_kernel_ptr_##N();
+        PSB_NCP_LIST(PSB_CASE)
+#undef PSB_CASE
+    default:
+        return nullptr;
+    }
+}
+
+static int prepare_kernel(const DevObject &o, KernelFn *fn, size_t *smem)
+{
+    *fn = kernel_for(o.ncp);
+    if (!*fn) return (int)cudaErrorInvalidValue;
+    *smem = fit_smem_bytes(o.n_fac, o.mfit);
+    cudaError_t e = cudaFuncSetAttribute(*fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
+    return (int)e;
+}
+
+int fit_ctas_per_sm(const DevObject &o)
+{
+    KernelFn fn;
+    size_t smem;
+    if (prepare_kernel(o, &fn, &smem) != 0) return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kThreads, smem) != cudaSuccess) return 0;
+    return n;
+}
+
+int launch_fits(const DevObject &o, const DevParams &p, const FitItem *items, int n_items, int *queue,
+                FitOut *out, double *scratch, size_t scratch_per_cta, int n_ctas, int *status, void *stream)
+{
+    KernelFn fn;
+    size_t smem;
+    int e = prepare_kernel(o, &fn, &smem);
+    if (e) return e;
+    EvalOut ev{};
+    fn<<<n_ctas, kThreads, smem, (cudaStream_t)stream>>>(o, p, items, n_items, queue, out, scratch,
+                                                         scratch_per_cta, status, ev, 0);
+    return (int)cudaGetLastError();
+}
+
+int launch_eval(const DevObject &o, const DevParams &p, EvalOut ev, double *scratch, void *stream)
+{
+    KernelFn fn;
+    size_t smem;
+    int e = prepare_kernel(o, &fn, &smem);
+    if (e) return e;
+    fn<<<1, kThreads, smem, (cudaStream_t)stream>>>(o, p, nullptr, 1, nullptr, nullptr, scratch, 0, nullptr,
+                                                    ev, 1);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace psb

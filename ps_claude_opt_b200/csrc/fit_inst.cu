@@ -1,0 +1,18 @@
+// fit_inst.cu -- one instance of the fit kernel, compiled once per padded
+// coefficient count (-DPSB_NCP=16..88) so the instances build in parallel.
+#include "fit_kernel.cuh"
+
+#ifndef PSB_NCP
+#error "compile with -DPSB_NCP=<padded coefficient count>"
+#endif
+
+namespace psb {
+
+using KernelFn = void (*)(DevObject, DevParams, const FitItem *, int, int *, FitOut *, double *, size_t,
+                          int *, EvalOut, int);
+
+#define PSB_CAT2(a, b) a##b
+#define PSB_CAT(a, b) PSB_CAT2(a, b)
+KernelFn PSB_CAT(fit_kernel_ptr_, PSB_NCP)() { return fit_kernel<PSB_NCP>; }
+
+}  // namespace psb

@@ -1,0 +1,277 @@
+"""ctypes binding of the native library ``_lib/libps_b200.so`` (include/ps_b200.h).
+
+There is no Python or CPU fallback: if the library is missing or a CUDA call
+fails, the call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libps_b200.so")
+
+N_POLES = 10
+QUIRK_PRECALC_CONW = 1
+DEVSTAT_SINGULAR = 1
+DEVSTAT_NAN_CHISQ = 2
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+class Curves(C.Structure):
+    _fields_ = [("n_curves", C.c_int32), ("curve_len", _ip), ("curve_rel", _ip)]
+
+
+class Shape(C.Structure):
+    _fields_ = [("n_coef", C.c_int32), ("normal", _dp), ("d_area", _dp), ("d_sphere", _dp)]
+
+
+class Line(C.Structure):
+    _fields_ = [("period_h", C.c_double), ("rms", C.c_double), ("chisq", C.c_double),
+                ("dark", C.c_double), ("lambda_deg", C.c_double), ("beta_deg", C.c_double)]
+
+
+class FitResult(C.Structure):
+    _fields_ = [("dev", C.c_double), ("dark", C.c_double), ("per", C.c_double),
+                ("lambda_deg", C.c_double), ("beta_deg", C.c_double), ("chisq", C.c_double),
+                ("niter", C.c_int32), ("status", C.c_int32)]
+
+
+PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int32)
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "ps_gpu_prepare": (C.c_int, [C.c_int32, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_double,
+                                 _dp, _dp, _dp, C.c_double, C.c_int32, _dp, C.POINTER(C.c_void_p)]),
+    "ps_gpu_precalc": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32, _dp,
+                                 C.c_int32, _ip, _ip, _ip, _dp, _dp, _dp, C.c_int32, _dp,
+                                 C.POINTER(Curves), C.POINTER(Shape)]),
+    "ps_gpu_start": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32,
+                               C.c_double, C.c_int32, _ip, _ip, _dp, C.c_double, _dp, _dp, C.c_int32, _dp,
+                               C.POINTER(Curves), C.POINTER(Shape), C.POINTER(Line), C.c_int32, _ip,
+                               PROGRESS_FN, C.c_void_p]),
+    "ps_gpu_unprepare": (None, [C.c_void_p]),
+    "ps_gpu_configure": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_double,
+                                   C.c_double, C.c_int32, _ip, _ip, _dp, _dp, _dp, C.c_int32, _dp,
+                                   C.POINTER(Curves), C.POINTER(Shape)]),
+    "ps_gpu_fit_items": (C.c_int, [C.c_void_p, C.c_int32, _ip, _ip, C.POINTER(FitResult)]),
+    "ps_gpu_fit_items_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "ps_gpu_eval": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
+    "ps_gpu_status": (C.c_int, [C.c_void_p, _ip]),
+    "ps_gpu_set_quirks": (C.c_int, [C.c_void_p, C.c_int32]),
+    "ps_gpu_stream": (C.c_void_p, [C.c_void_p]),
+    "ps_gpu_occupancy": (C.c_int, [C.c_void_p, _ip, _ip]),
+    "ps_setup_shape": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                 _dp, _dp, _dp, _dp]),
+    "ps_n_coef": (C.c_int32, [C.c_int32, C.c_int32]),
+    "ps_last_error": (C.c_char_p, []),
+    "ps_version": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded native library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"native library missing: {LIB_PATH} (run __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+class PsError(RuntimeError):
+    pass
+
+
+def _check(rc):
+    if rc != 0:
+        raise PsError(f"ps_b200 error {rc}: {lib().ps_last_error().decode()}")
+
+
+def _p(a, ct=C.c_double):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def setup_shape(l_max, m_max, nrows, a, b, c):
+    """Gaussian-image tables (normals, areas, Laplace basis, ellipsoid fit)."""
+    nfac = 8 * nrows * nrows
+    nc = int(lib().ps_n_coef(l_max, m_max))
+    normal = np.zeros((nfac, 3))
+    d_area = np.zeros(nfac)
+    dsph = np.zeros((nfac, nc))
+    cg = np.zeros(nc)
+    _check(lib().ps_setup_shape(l_max, m_max, nrows, a, b, c, _p(normal), _p(d_area), _p(dsph), _p(cg)))
+    return normal, d_area, dsph, cg
+
+
+class Engine:
+    """One prepared object on one GPU (the reference's CUDAPrepare state)."""
+
+    def __init__(self, obj, device: int = 0):
+        self.obj = obj
+        self._keep = []
+        L = lib()
+        h = C.c_void_p()
+        self._ee = self._arr(obj.ee)
+        self._ee0 = self._arr(obj.ee0)
+        self._tim = self._arr(obj.tim)
+        _check(L.ps_gpu_prepare(device, _p(self._arr(obj.beta_pole)), _p(self._arr(obj.lambda_pole)),
+                                _p(self._arr(obj.par)), float(obj.cl), obj.alamda_start,
+                                obj.alamda_incr, obj.alamda_incrr, _p(self._ee), _p(self._ee0), _p(self._tim),
+                                obj.phi0, obj.n_points, _p(self._arr(obj.weight)), C.byref(h)))
+        self.h = h
+        self._ia = self._arr(obj.ia, np.int32)
+        self._ia_par = self._arr(obj.ia[obj.n_coef + 4:obj.n_coef + 7], np.int32)
+        self._cg = self._arr(obj.cg_first)
+        self._sig = self._arr(obj.sig)
+        self._sigr2 = self._arr(obj.sigr2)
+        self._br = self._arr(obj.brightness)
+        self.curves = Curves(obj.n_curves, _p(self._arr(obj.curve_len, np.int32), C.c_int32),
+                             _p(self._arr(obj.curve_rel, np.int32), C.c_int32))
+        self.shape = Shape(obj.n_coef, _p(self._arr(obj.normal)), _p(self._arr(obj.d_area)),
+                           _p(self._arr(obj.dsph)))
+
+    def _arr(self, x, dt=np.float64):
+        a = np.ascontiguousarray(x, dtype=dt)
+        self._keep.append(a)
+        return a
+
+    def close(self):
+        if self.h:
+            lib().ps_gpu_unprepare(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_quirks(self, q):
+        _check(lib().ps_gpu_set_quirks(self.h, q))
+
+    def configure(self, conw_r=None, conw_r_rms=None, stop_condition=None, grid=None):
+        o = self.obj
+        g = grid or o.grid
+        cw = o.conw_r if conw_r is None else conw_r
+        stop = stop_condition if stop_condition is not None else self._stop()
+        _check(lib().ps_gpu_configure(self.h, g.freq_start, g.freq_step, stop, o.n_iter_min, cw,
+                                      cw if conw_r_rms is None else conw_r_rms, o.n_points,
+                                      _p(self._ia, C.c_int32), _p(self._ia_par, C.c_int32), _p(self._cg),
+                                      _p(self._sig), _p(self._sigr2), o.n_fac, _p(self._br),
+                                      C.byref(self.curves), C.byref(self.shape)))
+
+    def _stop(self):
+        return float(self.obj.stop_condition)
+
+    def fit_items(self, n_freq, pole):
+        n_freq = np.ascontiguousarray(n_freq, dtype=np.int32)
+        pole = np.ascontiguousarray(pole, dtype=np.int32)
+        n = len(n_freq)
+        res = (FitResult * max(n, 1))()
+        _check(lib().ps_gpu_fit_items(self.h, n, _p(n_freq, C.c_int32), _p(pole, C.c_int32), res))
+        out = np.array([(r.dev, r.dark, r.per, r.lambda_deg, r.beta_deg, r.chisq) for r in res[:n]])
+        niter = np.array([r.niter for r in res[:n]], dtype=np.int32)
+        status = np.array([r.status for r in res[:n]], dtype=np.int32)
+        return out.reshape(n, 6), niter, status
+
+    def fit_items_device(self, n, d_items_ptr, d_out_ptr):
+        _check(lib().ps_gpu_fit_items_device(self.h, n, C.c_void_p(d_items_ptr), C.c_void_p(d_out_ptr)))
+
+    def eval(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        mf = self.obj.mfit
+        alpha = np.zeros((mf, mf))
+        beta = np.zeros(mf)
+        chisq = np.zeros(1)
+        area = np.zeros(1)
+        _check(lib().ps_gpu_eval(self.h, _p(a), _p(chisq), _p(alpha), _p(beta), _p(area)))
+        return float(chisq[0]), alpha, beta, float(area[0])
+
+    def precalc(self, conw_r, grid=None):
+        o = self.obj
+        g = grid or o.grid
+        cw = np.array([conw_r], dtype=np.float64)
+        nc = np.zeros(1, dtype=np.int32)
+        _check(lib().ps_gpu_precalc(self.h, g.freq_start, g.freq_end, g.freq_step, self._stop(), o.n_iter_min,
+                                    _p(cw), o.n_points, _p(self._ia, C.c_int32), _p(self._ia_par, C.c_int32),
+                                    _p(nc, C.c_int32), _p(self._cg), _p(self._sig), _p(self._sigr2), o.n_fac,
+                                    _p(self._br), C.byref(self.curves), C.byref(self.shape)))
+        return float(cw[0]), int(nc[0])
+
+    def start(self, conw_r, n_start_from=1, max_lines=None, grid=None, progress=None):
+        o = self.obj
+        g = grid or o.grid
+        cap = g.n_max - n_start_from + 1 if max_lines is None else max_lines
+        lines = (Line * max(cap, 1))()
+        nl = np.zeros(1, dtype=np.int32)
+        cb = PROGRESS_FN(progress) if progress else PROGRESS_FN()
+        _check(lib().ps_gpu_start(self.h, n_start_from, g.freq_start, g.freq_end, g.freq_step, self._stop(),
+                                  o.n_iter_min, conw_r, o.n_points, _p(self._ia, C.c_int32),
+                                  _p(self._ia_par, C.c_int32), _p(self._cg), o.escl, _p(self._sig),
+                                  _p(self._sigr2), o.n_fac, _p(self._br), C.byref(self.curves),
+                                  C.byref(self.shape), lines, cap, _p(nl, C.c_int32), cb, None))
+        n = int(nl[0])
+        return np.array([(l.period_h, l.rms, l.chisq, l.dark, l.lambda_deg, l.beta_deg) for l in lines[:n]])
+
+    def status(self):
+        f = np.zeros(1, dtype=np.int32)
+        _check(lib().ps_gpu_status(self.h, _p(f, C.c_int32)))
+        return int(f[0])
+
+    def occupancy(self):
+        a = np.zeros(1, dtype=np.int32)
+        b = np.zeros(1, dtype=np.int32)
+        _check(lib().ps_gpu_occupancy(self.h, _p(a, C.c_int32), _p(b, C.c_int32)))
+        return int(a[0]), int(b[0])
+
+    @property
+    def stream(self):
+        return lib().ps_gpu_stream(self.h)
+
+
+def run_object(obj, device=0, quirks=0, max_freq=None, progress=None):
+    """The reference's main flow after parsing: conw precalc loop, then the scan.
+    Returns (lines, final conw_r)."""
+    with Engine(obj, device) as eng:
+        eng.set_quirks(quirks)
+        conw_r = obj.conw_r
+        new_conw = 0
+        while new_conw != 1 and conw_r * obj.escl * obj.escl < 10.0:
+            conw_r, new_conw = eng.precalc(conw_r)
+        lines = eng.start(conw_r, max_lines=max_freq, progress=progress)
+    return lines, conw_r
+
+
+def format_lines(lines):
+    """period_search_out text (start_CUDA.cu:1220-1227)."""
+    out = []
+    for l in lines:
+        out.append("%.8f  %.6f  %.6f %4.1f %4.0f %4.0f\n" % (l[0], l[1], l[2], l[3], _round(l[4]), _round(l[5])))
+    return "".join(out)
+
+
+def _round(x):
+    # C round(): half away from zero
+    return float(np.sign(x) * np.floor(abs(x) + 0.5))

@@ -1,0 +1,44 @@
+import functools
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+@functools.lru_cache(maxsize=None)
+def synth_text(kind: str, seed: int):
+    from ps_claude_opt_b200 import synth
+
+    cfgs = {
+        # tiny: seconds on the oracle
+        "tiny": synth.SynthConfig(l_max=3, m_max=3, nrows=4, n_dense=4, dense_pts=(24, 24), n_freq=6),
+        # C1 shape (lmax 3, nrows 6, 20 x 60 relative points), 8 trial frequencies
+        "c1": synth.SynthConfig(n_freq=8),
+        # mixed relative + calibrated, lmax 4 (ia[1] fitted)
+        "mixed": synth.SynthConfig(l_max=4, m_max=4, nrows=5, n_dense=6, dense_pts=(20, 40), n_sparse=60,
+                                   sparse_curves=2, n_freq=6),
+        # C2 shape (lmax 6, nrows 8, 40 dense + 400 calibrated points), few frequencies
+        "c2": synth.SynthConfig(l_max=6, m_max=6, nrows=8, n_dense=40, dense_pts=(50, 120), n_sparse=400,
+                                sparse_curves=2, n_freq=4),
+    }
+    text, truth = synth.generate(cfgs[kind], seed)
+    return text, truth
+
+
+def prepared(kind: str, seed: int = 11, setup="oracle"):
+    from ps_claude_opt_b200 import objects
+
+    text, _ = synth_text(kind, seed)
+    if setup == "oracle":
+        import oracle
+
+        return objects.parse_input(text, setup_fn=oracle.setup_shape)
+    return objects.parse_input(text)
