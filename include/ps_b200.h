@@ -165,6 +165,10 @@ ps_status ps_setup_shape(int32_t l_max, int32_t m_max, int32_t nrows, double a, 
                          double *normal, double *d_area, double *d_sphere, double *cg_first);
 int32_t ps_n_coef(int32_t l_max, int32_t m_max);
 
+/* FP64 FMA throughput of the device in TFLOP/s (the compute roofline of the
+   fit kernel; no reference counterpart). */
+ps_status ps_measure_fp64_peak(int32_t device, double *tflops);
+
 const char *ps_last_error(void);
 const char *ps_version(void);
 

@@ -1,0 +1,64 @@
+// probe.cu -- FP64 FMA throughput probe: the compute roofline denominator of
+// the fit kernel.  Independent FMA chains per thread, enough warps per SM to
+// keep the FP64 pipe busy; returns achieved TFLOP/s (2 FLOP per FMA).
+#include <cuda_runtime.h>
+
+#include "ps_b200.h"
+#include "util.h"
+
+namespace {
+
+constexpr int kChains = 8;
+constexpr int kIters = 4096;
+
+__global__ void __launch_bounds__(256) fma_probe(double *out, double x)
+{
+    double a[kChains];
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) a[c] = x + threadIdx.x * 1e-9 + c;
+    const double m = 0.999999, s = 1e-7;
+#pragma unroll 4
+    for (int i = 0; i < kIters; ++i)
+#pragma unroll
+        for (int c = 0; c < kChains; ++c) a[c] = fma(a[c], m, s);
+    double t = 0;
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) t += a[c];
+    if (t == 12345.678) out[blockIdx.x] = t;  // never true; keeps the work live
+}
+
+}  // namespace
+
+extern "C" ps_status ps_measure_fp64_peak(int32_t device, double *tflops)
+{
+    if (!tflops) return psb_fail(PS_ERR_ARG, "ps_measure_fp64_peak: null argument");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return psb_fail_cuda(e, "cudaSetDevice");
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) return psb_fail_cuda(e, "cudaGetDeviceProperties");
+    const int blocks = prop.multiProcessorCount * 8;
+    double *out = nullptr;
+    if ((e = cudaMalloc(&out, sizeof(double) * blocks)) != cudaSuccess) return psb_fail_cuda(e, "cudaMalloc");
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    fma_probe<<<blocks, 256>>>(out, 1.0);  // warm-up
+    float best_ms = 1e30f;
+    for (int r = 0; r < 5; ++r) {
+        cudaEventRecord(t0);
+        fma_probe<<<blocks, 256>>>(out, 1.0 + r);
+        cudaEventRecord(t1);
+        cudaEventSynchronize(t1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, t0, t1);
+        if (ms < best_ms) best_ms = ms;
+    }
+    e = cudaGetLastError();
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    cudaFree(out);
+    if (e != cudaSuccess) return psb_fail_cuda(e, "fma_probe");
+    const double flop = 2.0 * kChains * (double)kIters * 256.0 * blocks;
+    *tflops = flop / (best_ms * 1e-3) / 1e12;
+    return PS_OK;
+}

@@ -68,6 +68,7 @@ _SIGS = {
     "ps_setup_shape": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                  _dp, _dp, _dp, _dp]),
     "ps_n_coef": (C.c_int32, [C.c_int32, C.c_int32]),
+    "ps_measure_fp64_peak": (C.c_int, [C.c_int32, _dp]),
     "ps_last_error": (C.c_char_p, []),
     "ps_version": (C.c_char_p, []),
 }
@@ -117,6 +118,12 @@ def setup_shape(l_max, m_max, nrows, a, b, c):
     cg = np.zeros(nc)
     _check(lib().ps_setup_shape(l_max, m_max, nrows, a, b, c, _p(normal), _p(d_area), _p(dsph), _p(cg)))
     return normal, d_area, dsph, cg
+
+
+def measure_fp64_peak(device=0):
+    t = np.zeros(1)
+    _check(lib().ps_measure_fp64_peak(device, _p(t)))
+    return float(t[0])
 
 
 class Engine:
