@@ -17,6 +17,7 @@ data-path collective); the timing is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -225,7 +226,8 @@ def main():
 
     stream = torch.cuda.ExternalStream(eng.stream)
     d_items = [torch.from_numpy(items_for(s)).cuda() for s in range(steps_total)]
-    d_out = torch.empty(n_fits * 48, dtype=torch.uint8, device="cuda")
+    rec = ctypes.sizeof(native.FitResult)   # one ps_fit_result per fit
+    d_out = torch.empty(n_fits * rec, dtype=torch.uint8, device="cuda")
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
 
@@ -265,6 +267,7 @@ def main():
     res = np.frombuffer(d_out.cpu().numpy().tobytes(), dtype=np.dtype(
         [("dev", "f8"), ("dark", "f8"), ("per", "f8"), ("la", "f8"), ("be", "f8"), ("chisq", "f8"),
          ("niter", "i4"), ("status", "i4")]))
+    assert res.dtype.itemsize == rec
     niter = float(np.mean(res["niter"]))
     if not np.all(np.isfinite(res["per"])):
         raise RuntimeError("non-finite fit results")
@@ -282,7 +285,7 @@ def main():
     it = items_for(args.warmup)
     h2d = (obj.n_points * (4 * 8 + 4 * 8 + 8 + 4) + obj.n_fac * (32 + 8 * ((obj.n_coef + 7) // 8 * 8))
            + it.nbytes)
-    d2h = n_fits * 48
+    d2h = n_fits * rec
     e2e_ms = []
     for s in range(max(1, min(args.steps, 3))):
         flush.fill_(s)

@@ -47,6 +47,8 @@ typedef enum ps_status {
 /* Device-status bits accumulated over calls (ps_gpu_status). */
 #define PS_DEVSTAT_SINGULAR 1   /* a Gauss-Jordan pivot was exactly zero */
 #define PS_DEVSTAT_NAN_CHISQ 2  /* an evaluation produced NaN chi^2 */
+#define PS_DEVSTAT_TIMEOUT 4    /* a bounded wait for a shared-memory bulk copy gave up;
+                                   the CTA stopped and its remaining items are unset */
 
 /* Quirk bits (ps_gpu_set_quirks): reproduce documented reference behaviour. */
 #define PS_QUIRK_PRECALC_CONW 1 /* start_CUDA.cu:476 uploads the pointer bits of

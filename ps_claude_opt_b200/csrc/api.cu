@@ -200,7 +200,7 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
 
     cudaDeviceProp prop;
     PSB_CUDA(cudaGetDeviceProperties(&prop, h->device));
-    const size_t smem = psb::fit_smem_bytes(numfac, mfit);
+    const size_t smem = psb::fit_smem_bytes(numfac, mfit, ncp);
     if (smem > prop.sharedMemPerBlockOptin)
         return psb_fail(PS_ERR_ARG, "ps_gpu_configure: object too large for shared memory");
 

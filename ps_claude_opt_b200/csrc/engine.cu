@@ -21,11 +21,12 @@ int padded_ncoef(int n_coef)
     return -1;
 }
 
-size_t fit_smem_bytes(int n_fac, int mfit) { return carve_bytes(n_fac, mfit, nullptr, nullptr); }
+size_t fit_smem_bytes(int n_fac, int mfit, int ncp) { return carve_bytes(n_fac, mfit, ncp, nullptr, nullptr); }
 
 size_t fit_scratch_doubles(const DevObject &o)
 {
-    size_t n = (size_t)o.n_points * o.row_stride + (size_t)o.n_curves * (o.ma + 3);
+    // derivative rows, per-curve statistics, point order + sort keys (2 ints per point)
+    size_t n = (size_t)o.n_points * o.row_stride + (size_t)o.n_curves * (o.ma + 3) + (size_t)o.n_points;
     return (n + 31) & ~size_t(31);
 }
 
@@ -51,7 +52,7 @@ static int prepare_kernel(const DevObject &o, KernelFn *fn, size_t *smem)
 {
     *fn = kernel_for(o.ncp);
     if (!*fn) return (int)cudaErrorInvalidValue;
-    *smem = fit_smem_bytes(o.n_fac, o.mfit);
+    *smem = fit_smem_bytes(o.n_fac, o.mfit, o.ncp);
     cudaError_t e = cudaFuncSetAttribute(*fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
     return (int)e;
 }

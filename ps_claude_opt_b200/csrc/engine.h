@@ -62,10 +62,11 @@ struct EvalOut {
 enum StatusBits : int {
     kStatusSingular = 1,
     kStatusNanChisq = 2,
+    kStatusTimeout = 4,   // a bounded wait on a bulk copy gave up
 };
 
 // Bytes of dynamic shared memory one fit CTA needs.
-size_t fit_smem_bytes(int n_fac, int mfit);
+size_t fit_smem_bytes(int n_fac, int mfit, int ncp);
 // Doubles of scratch one CTA needs (derivative rows + per-curve statistics).
 size_t fit_scratch_doubles(const DevObject &o);
 // Padded coefficient count the kernels are compiled for.

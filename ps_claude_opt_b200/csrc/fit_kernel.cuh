@@ -28,10 +28,15 @@ namespace psb {
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kTiny = 1e-8;
 constexpr int kBPT = 5;  // 2x2 alpha blocks per thread: ceil(45*46/2 / 256)
+constexpr int kFacetChunk = 32;     // facets per shared-memory basis chunk
+constexpr int kSortBands = 8;       // point sort: bands in cos(theta) ...
+constexpr int kSortSectors = 32;    // ... x sectors in longitude of the Sun-observer bisector
+constexpr int kSortCells = kSortBands * kSortSectors;
+constexpr unsigned kWaitLimit = 1u << 24;  // bounded mbarrier waits
 
 // LM scalar slots in shared memory
 enum { S_ALAMDA, S_CHISQ, S_OCHISQ, S_ITERDIFF, S_DEVOLD, S_DEVNEW, S_CHCK, S_AREA, S_TRIAL, S_PIVINV, S_NSCAL };
-enum { C_ITEM, C_NITER, C_STATUS, C_ERR, C_IROW, C_ICOL, C_GO, C_ACCEPT, C_NCTL };
+enum { C_ITEM, C_NITER, C_STATUS, C_ERR, C_IROW, C_ICOL, C_GO, C_ACCEPT, C_YUSE0, C_YUSE1, C_TIMEOUT, C_NCTL };
 
 struct Sh {
     double4 *F;       // [n_fac] normal + current area
@@ -41,8 +46,11 @@ struct Sh {
     double *da;       // [kMaxFit]
     double *a;        // [kMaxPar]
     double *atry;     // [kMaxPar]
-    double *T;        // [kTile][mfp]
-    double *TW;       // [kTile][mfp]
+    double *T;        // [kTile][mfp]       (shares storage with ybuf)
+    double *TW;       // [kTile][mfp]       (shares storage with ybuf)
+    double *ybuf;     // [2][kFacetChunk][ncp] basis chunks of the facet sweep
+    unsigned long long *mbar;  // [2] completion barriers of the chunk copies
+    int *hist;        // [2][kSortCells] point-sort histogram and offsets
     double *rdy;      // [kTile]
     double *rw;       // [kTile]
     double *red;      // [kWarps * 4]
@@ -62,12 +70,54 @@ __device__ __forceinline__ double4 ldg4(const double4 *p)
     return make_double4(a.x, a.y, b.x, b.y);
 }
 
+// ---------------------------------------------------------------- bulk copies
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// One-thread producer: expect `bytes` on bar, then copy them global -> shared
+// with the bulk-copy engine (cp.async.bulk, no cluster multicast).
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, unsigned long long *bar)
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Waits for the phase with the given parity to complete; gives up after
+// kWaitLimit polls and returns false (the caller records a timeout).
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity)
+{
+    for (unsigned i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 __host__ __device__ inline int fit_ld(int mfit) { return mfit | 1; }
 __host__ __device__ inline int fit_mfp(int mfit) { return (mfit + 1) & ~1; }
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-__host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, Sh *s, unsigned char *base)
+__host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, Sh *s, unsigned char *base)
 {
     int ld = fit_ld(mfit), mfp = fit_mfp(mfit);
     size_t off = 0;
@@ -83,8 +133,16 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, Sh *s, unsign
     void *da = take(sizeof(double) * kMaxFit);
     void *a = take(sizeof(double) * kMaxPar);
     void *atry = take(sizeof(double) * kMaxPar);
-    void *T = take(sizeof(double) * kTile * mfp);
-    void *TW = take(sizeof(double) * kTile * mfp);
+    // the JtWJ tiles (phase D) and the basis chunks (phase B) are never live
+    // at the same time: one region serves both
+    const size_t tiles = 2 * align16(sizeof(double) * kTile * mfp);
+    const size_t chunks = 2 * sizeof(double) * kFacetChunk * ncp;
+    unsigned char *un = (unsigned char *)take(tiles > chunks ? tiles : chunks);
+    void *T = un;
+    void *TW = un ? un + align16(sizeof(double) * kTile * mfp) : nullptr;
+    void *ybuf = un;
+    void *mbar = take(sizeof(unsigned long long) * 2);
+    void *hist = take(sizeof(int) * 2 * kSortCells);
     void *rdy = take(sizeof(double) * kTile);
     void *rw = take(sizeof(double) * kTile);
     void *red = take(sizeof(double) * kWarps * 4);
@@ -98,6 +156,7 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, Sh *s, unsign
         s->F = (double4 *)F; s->alpha = (double *)alpha; s->covar = (double *)covar;
         s->beta = (double *)beta; s->da = (double *)da; s->a = (double *)a; s->atry = (double *)atry;
         s->T = (double *)T; s->TW = (double *)TW; s->rdy = (double *)rdy; s->rw = (double *)rw;
+        s->ybuf = (double *)ybuf; s->mbar = (unsigned long long *)mbar; s->hist = (int *)hist;
         s->red = (double *)red; s->inv = (double *)inv; s->scal = (double *)scal;
         s->colbuf = (double *)colbuf; s->fidx = (int *)fidx; s->ipiv = (int *)ipiv; s->ctl = (int *)ctl;
         s->ld = ld; s->mfp = mfp;
@@ -255,94 +314,201 @@ __device__ __forceinline__ void point_geometry(const double *inv, double t, cons
     }
 }
 
+// Order of the points for the facet sweep: counting sort on the body-frame
+// direction of the Sun-observer bisector, so the 32 points of a warp see
+// nearly the same facets and whole warps skip facets none of them sees.  Rows
+// are written at the original point index and every skipped term is an exact
+// zero, so the order changes nothing in the results.
+static __device__ void sort_points(const DevObject &o, const Sh &s, int *perm, int *keys)
+{
+    const int tid = threadIdx.x, np = o.n_points;
+    int *hist = s.hist, *offs = s.hist + kSortCells;
+    for (int c = tid; c < kSortCells; c += kThreads) hist[c] = 0;
+    __syncthreads();
+    for (int q = tid; q < np; q += kThreads) {
+        const double4 pa = ldg4(&o.pt_a[q]);
+        const double4 pb = ldg4(&o.pt_b[q]);
+        const double ee[3] = {pa.y, pa.z, pa.w}, es[3] = {pb.x, pb.y, pb.z};
+        PointGeo g;
+        point_geometry<false>(s.inv, pa.x, ee, es, g);
+        const double bx = g.e[0] + g.e0[0], by = g.e[1] + g.e0[1], bz = g.e[2] + g.e0[2];
+        const double n = sqrt(bx * bx + by * by + bz * bz);
+        const double cz = n > 0 ? bz / n : 0.0;
+        int band = (int)((cz + 1.0) * (0.5 * kSortBands));
+        band = min(max(band, 0), kSortBands - 1);
+        // pseudo-angle of (bx, by) in [0, 4): monotone in longitude, no trig
+        const double ax = fabs(bx), ay = fabs(by), sum = ax + ay;
+        double pa4 = sum > 0 ? ay / sum : 0.0;
+        if (bx < 0) pa4 = 2.0 - pa4;
+        if (by < 0) pa4 = 4.0 - pa4;
+        int sec = (int)(pa4 * (0.25 * kSortSectors));
+        sec = min(max(sec, 0), kSortSectors - 1);
+        const int key = band * kSortSectors + ((band & 1) ? kSortSectors - 1 - sec : sec);
+        keys[q] = key;
+        atomicAdd(&hist[key], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x, per = kSortCells / 32;
+        int local[kSortCells / 32], sum = 0;
+#pragma unroll
+        for (int i = 0; i < per; ++i) {
+            local[i] = hist[lane * per + i];
+            sum += local[i];
+        }
+        int incl = sum;
+#pragma unroll
+        for (int o2 = 1; o2 < 32; o2 <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o2);
+            if (lane >= o2) incl += v;
+        }
+        int run = incl - sum;
+#pragma unroll
+        for (int i = 0; i < per; ++i) {
+            offs[lane * per + i] = run;
+            run += local[i];
+        }
+    }
+    __syncthreads();
+    for (int q = tid; q < np; q += kThreads) perm[atomicAdd(&offs[keys[q]], 1)] = q;
+    __syncthreads();
+}
+
 // Brightness and raw derivative rows of all points: mrqcof_curve1_opt
 // (Start.cu:2262-2535).  Row layout: column p-1 = d ymod / d a_p for
 // p = 1..ma, column ma = ymod (un-renormalised).
+//
+// All warps sweep the facets in lockstep, kFacetChunk facets at a time; the
+// chunk's basis rows (ncp doubles each) arrive in shared memory by bulk copy,
+// double-buffered, so the shape-derivative loop reads broadcast shared-memory
+// operands.  One warp = 32 points (lane = point), shape-derivative sums in
+// registers.
 template <int NCP>
-__device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows)
+__device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows, const int *perm)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int np = o.n_points, nf = o.n_fac, nc = o.n_coef, RS = o.row_stride;
     const double cl = s.inv[5], cls = s.inv[6];
+    const int nchunks = (nf + kFacetChunk - 1) / kFacetChunk;
+    const int ntiles = (np + 31) / 32;
+    const int nrounds = (ntiles + kWarps - 1) / kWarps;
+    const int total = nrounds * nchunks;
+    int use[2] = {s.ctl[C_YUSE0], s.ctl[C_YUSE1]};  // completed waits per buffer (parity source)
+    bool timeout = false;
 
-    for (int tile = warp; tile * 32 < np; tile += kWarps) {
-        const int p = tile * 32 + lane;
-        const bool act = p < np;
-        const int pc = act ? p : np - 1;
-        double t, ee[3], es[3];
+    auto issue = [&](int g) {
+        const int c = g % nchunks, f0 = c * kFacetChunk;
+        const int rows_c = min(kFacetChunk, nf - f0);
+        const int b = g & 1;
+        bulk_load(s.ybuf + (size_t)b * kFacetChunk * NCP, o.ysh + (size_t)f0 * NCP,
+                  (uint32_t)(rows_c * NCP * sizeof(double)), &s.mbar[b]);
+    };
+    if (tid == 0)
+        for (int g = 0; g < 2 && g < total; ++g) issue(g);
+
+    int g = 0;
+    for (int round = 0; round < nrounds; ++round) {
+        const int tile = round * kWarps + warp;
+        const bool tile_act = tile < ntiles;
+        const int idx = tile * 32 + lane;
+        const bool act = tile_act && idx < np;
+        const int p = perm[min(idx, np - 1)];
+        double t = 0, ee[3] = {0, 0, 0}, es[3] = {0, 0, 0};
         {
-            const double4 pa = ldg4(&o.pt_a[pc]);
-            const double4 pb = ldg4(&o.pt_b[pc]);
+            const double4 pa = ldg4(&o.pt_a[p]);
+            const double4 pb = ldg4(&o.pt_b[p]);
             t = pa.x;
             ee[0] = pa.y; ee[1] = pa.z; ee[2] = pa.w;
             es[0] = pb.x; es[1] = pb.y; es[2] = pb.z;
         }
-        PointGeo g;
-        point_geometry<false>(s.inv, t, ee, es, g);
-        const double e0x = g.e[0], e0y = g.e[1], e0z = g.e[2];
-        const double s0x = g.e0[0], s0y = g.e0[1], s0z = g.e0[2];
+        PointGeo geo;
+        point_geometry<false>(s.inv, t, ee, es, geo);
+        const double ex = geo.e[0], ey = geo.e[1], ez = geo.e[2];
+        const double sx = geo.e0[0], sy = geo.e0[1], sz = geo.e0[2];
 
         double J[NCP];
 #pragma unroll
         for (int k = 0; k < NCP; ++k) J[k] = 0.0;
         double br = 0, u0 = 0, u1 = 0, u2 = 0, w0 = 0, w1 = 0, w2 = 0, t4 = 0, t5 = 0;
 
+        for (int c = 0; c < nchunks; ++c, ++g) {
+            const int b = g & 1;
+            if (!mbar_wait(&s.mbar[b], (uint32_t)(use[b] & 1))) timeout = true;
+            if (tile_act) {
+                const int f0 = c * kFacetChunk, f1 = min(nf, f0 + kFacetChunk);
+                const double *yb = s.ybuf + (size_t)b * kFacetChunk * NCP;
 #pragma unroll 1
-        for (int fi = 0; fi < nf; ++fi) {
-            const double4 fr = s.F[fi];
-            const double mu = e0x * fr.x + e0y * fr.y + e0z * fr.z;
-            const double mu0 = s0x * fr.x + s0y * fr.y + s0z * fr.z;
-            const bool vis = act && (mu > kTiny) && (mu0 > kTiny);
-            if (__any_sync(0xffffffffu, vis)) {
-                const double ar = fr.w;
-                const double r = __drcp_rn(mu + mu0);
-                const double sv = mu * mu0 * (cl + cls * r);
-                const double q0 = mu0 * r, q1 = mu * r;
-                const double dsmu = cls * (q0 * q0) + cl * mu0;
-                const double dsmu0 = cls * (q1 * q1) + cl * mu;
-                const double amm = ar * mu * mu0;
-                const double w = vis ? ar * sv : 0.0;
-                const double gg = vis ? ar * dsmu : 0.0;
-                const double g0 = vis ? ar * dsmu0 : 0.0;
-                br += w;
-                u0 = fma(gg, fr.x, u0);
-                u1 = fma(gg, fr.y, u1);
-                u2 = fma(gg, fr.z, u2);
-                w0 = fma(g0, fr.x, w0);
-                w1 = fma(g0, fr.y, w1);
-                w2 = fma(g0, fr.z, w2);
-                t4 += vis ? amm : 0.0;
-                t5 += vis ? amm * r : 0.0;
-                const double2 *yr = reinterpret_cast<const double2 *>(o.ysh + (size_t)fi * NCP);
+                for (int fi = f0; fi < f1; ++fi) {
+                    const double4 fr = s.F[fi];
+                    const double mu = ex * fr.x + ey * fr.y + ez * fr.z;
+                    const double mu0 = sx * fr.x + sy * fr.y + sz * fr.z;
+                    const bool vis = act && (mu > kTiny) && (mu0 > kTiny);
+                    if (__any_sync(0xffffffffu, vis)) {
+                        // lanes that do not see the facet run the same arithmetic on
+                        // finite stand-ins and contribute exact zeros
+                        const double ar = vis ? fr.w : 0.0;
+                        const double r = __drcp_rn(vis ? mu + mu0 : 1.0);
+                        const double sv = mu * mu0 * (cl + cls * r);
+                        const double q0 = mu0 * r, q1 = mu * r;
+                        const double dsmu = cls * (q0 * q0) + cl * mu0;
+                        const double dsmu0 = cls * (q1 * q1) + cl * mu;
+                        const double amm = ar * mu * mu0;
+                        const double w = ar * sv;
+                        const double gg = ar * dsmu;
+                        const double g0 = ar * dsmu0;
+                        br += w;
+                        u0 = fma(gg, fr.x, u0);
+                        u1 = fma(gg, fr.y, u1);
+                        u2 = fma(gg, fr.z, u2);
+                        w0 = fma(g0, fr.x, w0);
+                        w1 = fma(g0, fr.y, w1);
+                        w2 = fma(g0, fr.z, w2);
+                        t4 += amm;
+                        t5 += amm * r;
+                        const double2 *yr = reinterpret_cast<const double2 *>(yb + (size_t)(fi - f0) * NCP);
 #pragma unroll
-                for (int k = 0; k < NCP / 2; ++k) {
-                    const double2 y = __ldg(yr + k);
-                    J[2 * k] = fma(w, y.x, J[2 * k]);
-                    J[2 * k + 1] = fma(w, y.y, J[2 * k + 1]);
+                        for (int k = 0; k < NCP / 2; ++k) {
+                            const double2 y = yr[k];
+                            J[2 * k] = fma(w, y.x, J[2 * k]);
+                            J[2 * k + 1] = fma(w, y.y, J[2 * k + 1]);
+                        }
+                    }
                 }
             }
+            __syncthreads();  // every warp is done with buffer b
+            use[b] += 1;
+            if (tid == 0 && g + 2 < total) issue(g + 2);
         }
 
-        point_geometry<true>(s.inv, t, ee, es, g);
-        const double t1 = (g.db[0] * u0 + g.db[1] * u1 + g.db[2] * u2) + (g.d0b[0] * w0 + g.d0b[1] * w1 + g.d0b[2] * w2);
-        const double t2 = (g.dl[0] * u0 + g.dl[1] * u1 + g.dl[2] * u2) + (g.d0l[0] * w0 + g.d0l[1] * w1 + g.d0l[2] * w2);
-        const double t3 = (g.dw[0] * u0 + g.dw[1] * u1) + (g.d0w[0] * w0 + g.d0w[1] * w1);
-        if (act) {
-            const double scale = g.scale;
-            double *row = rows + (size_t)p * RS;
+        if (tile_act) {
+            point_geometry<true>(s.inv, t, ee, es, geo);
+            const double t1 = (geo.db[0] * u0 + geo.db[1] * u1 + geo.db[2] * u2) +
+                              (geo.d0b[0] * w0 + geo.d0b[1] * w1 + geo.d0b[2] * w2);
+            const double t2 = (geo.dl[0] * u0 + geo.dl[1] * u1 + geo.dl[2] * u2) +
+                              (geo.d0l[0] * w0 + geo.d0l[1] * w1 + geo.d0l[2] * w2);
+            const double t3 = (geo.dw[0] * u0 + geo.dw[1] * u1) + (geo.d0w[0] * w0 + geo.d0w[1] * w1);
+            if (act) {
+                const double scale = geo.scale;
+                double *row = rows + (size_t)p * RS;
 #pragma unroll
-            for (int k = 0; k < NCP; ++k)
-                if (k < nc) row[k] = scale * J[k];
-            row[nc + 0] = scale * t1;
-            row[nc + 1] = scale * t2;
-            row[nc + 2] = scale * t3;
-            row[nc + 3] = br * g.ff;
-            row[nc + 4] = br * g.d2;
-            row[nc + 5] = br * g.alph;
-            row[nc + 6] = scale * t4 * cl;
-            row[nc + 7] = scale * t5;
-            row[nc + 8] = br * scale;
+                for (int k = 0; k < NCP; ++k)
+                    if (k < nc) row[k] = scale * J[k];
+                row[nc + 0] = scale * t1;
+                row[nc + 1] = scale * t2;
+                row[nc + 2] = scale * t3;
+                row[nc + 3] = br * geo.ff;
+                row[nc + 4] = br * geo.d2;
+                row[nc + 5] = br * geo.alph;
+                row[nc + 6] = scale * t4 * cl;
+                row[nc + 7] = scale * t5;
+                row[nc + 8] = br * scale;
+            }
         }
+    }
+    if (timeout) s.ctl[C_TIMEOUT] = 1;
+    if (tid == 0) {
+        s.ctl[C_YUSE0] = use[0];
+        s.ctl[C_YUSE1] = use[1];
     }
 }
 
@@ -409,7 +575,7 @@ __device__ __forceinline__ void tile_update(const Sh &s, int mfit, int nrows, Al
 // every thread.
 template <int NCP>
 __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, const double *a,
-                           double *dst, double *dvec, double *rows, double *cstat, double conw_r)
+                           double *dst, double *dvec, double *rows, double *cstat, int *perm, double conw_r)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ma = o.ma, mfit = o.mfit, mfp = s.mfp, RS = o.row_stride, CS = ma + 3;
@@ -418,7 +584,8 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
     if (tid == 0) s.scal[S_AREA] = area_sum;
     set_invariants(o, p, s, a);
 
-    brightness_rows<NCP>(o, s, rows);
+    sort_points(o, s, perm, perm + o.n_points);
+    brightness_rows<NCP>(o, s, rows, perm);
     __syncthreads();
 
     // per relative curve: column sums, 1/sum(ymod) and the renormalisation coefficient
@@ -693,20 +860,28 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Sh s;
-    carve_bytes(o.n_fac, o.mfit, &s, smem_raw);
+    carve_bytes(o.n_fac, o.mfit, o.ncp, &s, smem_raw);
     const int tid = threadIdx.x;
     const int nc = o.n_coef, ma = o.ma, mfit = o.mfit, ld = s.ld;
     double *rows = scratch + (size_t)blockIdx.x * scratch_per_cta;
     double *cstat = rows + (size_t)o.n_points * o.row_stride;
+    int *perm = reinterpret_cast<int *>(cstat + (size_t)o.n_curves * (ma + 3));  // [2][n_points]
 
     for (int f = tid; f < o.n_fac; f += kThreads) s.F[f] = ldg4(&o.facet[f]);
     if (tid < mfit) s.fidx[tid] = __ldg(&o.fidx[tid]);
+    if (tid == 0) {
+        mbar_init(&s.mbar[0], 1);
+        mbar_init(&s.mbar[1], 1);
+        s.ctl[C_YUSE0] = 0;
+        s.ctl[C_YUSE1] = 0;
+        s.ctl[C_TIMEOUT] = 0;
+    }
     __syncthreads();
 
     if (mode == 1) {  // one stand-alone evaluation (parity hook)
         for (int q = tid; q <= ma; q += kThreads) s.a[q] = ev.a[q];
         __syncthreads();
-        double chisq = evaluate<NCP>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, p.conw_r);
+        double chisq = evaluate<NCP>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, perm, p.conw_r);
         for (int idx = tid; idx < mfit * mfit; idx += kThreads) {
             const int j = idx / mfit, k = idx - j * mfit;
             ev.alpha[idx] = s.alpha[j * ld + k];
@@ -763,7 +938,7 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
             __syncthreads();
             if (first) {
                 if (tid == 0) s.scal[S_ALAMDA] = p.alamda_start;
-                double oc = evaluate<NCP>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, p.conw_r);
+                double oc = evaluate<NCP>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, perm, p.conw_r);
                 if (tid == 0) s.scal[S_OCHISQ] = oc;
                 for (int q = tid; q <= ma; q += kThreads) s.atry[q] = s.a[q];
                 __syncthreads();
@@ -783,7 +958,7 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
                 if (err == 2 && tid == 0) s.ctl[C_STATUS] |= kStatusSingular;
             }
             __syncthreads();
-            const double chisq = evaluate<NCP>(o, p, s, s.atry, s.covar, s.da, rows, cstat, p.conw_r);
+            const double chisq = evaluate<NCP>(o, p, s, s.atry, s.covar, s.da, rows, cstat, perm, p.conw_r);
             // accept / reject (mrqmin_2_end, Start.cu:300-392)
             const bool accept = chisq < s.scal[S_OCHISQ];
             __syncthreads();
@@ -849,11 +1024,18 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
             r.beta_deg = 90 - (180 / kPi) * s.a[nc + 1];
             r.chisq = s.scal[S_CHISQ];
             r.niter = s.ctl[C_NITER];
-            r.status = s.ctl[C_STATUS];
+            r.status = s.ctl[C_STATUS] | (s.ctl[C_TIMEOUT] ? kStatusTimeout : 0);
             out[item] = r;
             if (r.status) atomicOr(status, r.status);
         }
         __syncthreads();
+        if (s.ctl[C_TIMEOUT]) break;  // a bulk copy never completed: stop taking items
+    }
+    // after a timeout, give any copy still in flight a bounded chance to land
+    // before the CTA's shared memory is released
+    if (tid == 0 && s.ctl[C_TIMEOUT]) {
+        mbar_wait(&s.mbar[0], (uint32_t)(s.ctl[C_YUSE0] & 1));
+        mbar_wait(&s.mbar[1], (uint32_t)(s.ctl[C_YUSE1] & 1));
     }
 }
 
