@@ -156,6 +156,13 @@ ps_status ps_gpu_eval(ps_gpu *h, const double *a, double *chisq, double *alpha, 
 /* Device-status bits (PS_DEVSTAT_*) accumulated since prepare. */
 ps_status ps_gpu_status(ps_gpu *h, int32_t *flags);
 ps_status ps_gpu_set_quirks(ps_gpu *h, int32_t quirks);
+/* Per-phase SM clock totals of the fit kernel (diagnostics; no reference
+   counterpart).  If out is non-null it receives 12 values accumulated since
+   the last call -- cycles in curv, point sort, facet sweep, curve statistics,
+   J^T W J tiles (other), pseudo-points, Gauss-Jordan, the rest, tile-copy
+   waits, tile staging, tile rank-k updates, then the number of evaluations --
+   and the counters restart; enable = 0 switches them off. */
+ps_status ps_gpu_phase_clocks(ps_gpu *h, int32_t enable, int64_t *out);
 /* The CUDA stream all work of the handle runs on (a cudaStream_t). */
 void *ps_gpu_stream(ps_gpu *h);
 /* Fit CTAs resident per SM and SM count for the configured object. */

@@ -79,10 +79,11 @@ struct ps_gpu {
     psb::DevObject obj{};
     psb::DevParams prm{};
     int ctas_per_sm = 0;
-    DevBuf<double4> facet, pt_a, pt_b;
+    DevBuf<double4> facet, pt_a, pt_b, pt_rec;
     DevBuf<double> ysh, pt_w, curve_sig, cg_first, scratch, eval_buf;
     DevBuf<int> pt_curve, curve_start, curve_rel, fidx, queue, status;
     DevBuf<psb::FitItem> items;
+    DevBuf<unsigned long long> phase;
     DevBuf<psb::FitOut> out;
     size_t scratch_per_cta = 0;
 };
@@ -137,11 +138,11 @@ extern "C" void ps_gpu_unprepare(ps_gpu *h)
     if (!h) return;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    h->facet.release(); h->pt_a.release(); h->pt_b.release();
+    h->facet.release(); h->pt_a.release(); h->pt_b.release(); h->pt_rec.release();
     h->ysh.release(); h->pt_w.release(); h->curve_sig.release(); h->cg_first.release();
     h->scratch.release(); h->eval_buf.release();
     h->pt_curve.release(); h->curve_start.release(); h->curve_rel.release(); h->fidx.release();
-    h->queue.release(); h->status.release(); h->items.release(); h->out.release();
+    h->queue.release(); h->status.release(); h->items.release(); h->out.release(); h->phase.release();
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -200,7 +201,19 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
 
     cudaDeviceProp prop;
     PSB_CUDA(cudaGetDeviceProperties(&prop, h->device));
-    const size_t smem = psb::fit_smem_bytes(numfac, mfit, ncp);
+    // preferred layout first: 32-row tiles with the per-curve statistics in
+    // shared memory; fall back for the largest models
+    int tile_rows = 32, cstat_smem = 1;
+    const int rs = (ma + 2) & ~1;
+    size_t smem = psb::fit_smem_bytes(numfac, mfit, ncp, curves->n_curves, rs, tile_rows, cstat_smem);
+    if (smem > prop.sharedMemPerBlockOptin) {
+        cstat_smem = 0;
+        smem = psb::fit_smem_bytes(numfac, mfit, ncp, curves->n_curves, rs, tile_rows, cstat_smem);
+    }
+    if (smem > prop.sharedMemPerBlockOptin) {
+        tile_rows = 16;
+        smem = psb::fit_smem_bytes(numfac, mfit, ncp, curves->n_curves, rs, tile_rows, cstat_smem);
+    }
     if (smem > prop.sharedMemPerBlockOptin)
         return psb_fail(PS_ERR_ARG, "ps_gpu_configure: object too large for shared memory");
 
@@ -211,7 +224,7 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
     std::vector<double> ysh((size_t)numfac * ncp, 0.0);
     for (int f = 0; f < numfac; ++f)
         for (int k = 0; k < nc; ++k) ysh[(size_t)f * ncp + k] = shape->d_sphere[(size_t)f * nc + k];
-    std::vector<double4> pa(ndata), pb(ndata);
+    std::vector<double4> pa(ndata), pb(ndata), prec(ndata);
     std::vector<double> pw(ndata);
     std::vector<int> pcur(ndata), cstart(curves->n_curves + 1), crel(curves->n_curves);
     std::vector<double> csig(curves->n_curves);
@@ -225,6 +238,7 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
             pb[q] = make_double4(h->ee0[3 * q], h->ee0[3 * q + 1], h->ee0[3 * q + 2], brightness[q]);
             pw[q] = sigr2[q] * h->weight[q];
             pcur[q] = c;
+            prec[q] = make_double4(brightness[q], pw[q], (double)c, (double)crel[c]);
         }
     }
     cstart[curves->n_curves] = q;
@@ -236,6 +250,7 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
     PSB_CUDA(upload(h->pt_a, pa, s));
     PSB_CUDA(upload(h->pt_b, pb, s));
     PSB_CUDA(upload(h->pt_w, pw, s));
+    PSB_CUDA(upload(h->pt_rec, prec, s));
     PSB_CUDA(upload(h->pt_curve, pcur, s));
     PSB_CUDA(upload(h->curve_start, cstart, s));
     PSB_CUDA(upload(h->curve_rel, crel, s));
@@ -258,11 +273,14 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
     o.ma = ma;
     o.mfit = mfit;
     o.row_stride = (ma + 1 + 1) & ~1;
+    o.tile_rows = tile_rows;
+    o.cstat_smem = cstat_smem;
     o.facet = h->facet.ptr;
     o.ysh = h->ysh.ptr;
     o.pt_a = h->pt_a.ptr;
     o.pt_b = h->pt_b.ptr;
     o.pt_w = h->pt_w.ptr;
+    o.pt_rec = h->pt_rec.ptr;
     o.pt_curve = h->pt_curve.ptr;
     o.curve_start = h->curve_start.ptr;
     o.curve_rel = h->curve_rel.ptr;
@@ -300,6 +318,7 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
     p.conw_r_dev = conw_r_rms;
     p.freq_start = freq_start;
     p.freq_step = freq_step;
+    p.phase_cycles = h->phase.ptr;
 
     h->ctas_per_sm = psb::fit_ctas_per_sm(o);
     if (h->ctas_per_sm < 1) return psb_fail(PS_ERR_CUDA, "ps_gpu_configure: fit kernel cannot be resident");
@@ -397,6 +416,29 @@ extern "C" ps_status ps_gpu_eval(ps_gpu *h, const double *a, double *chisq, doub
     std::memcpy(beta, back.data() + (size_t)mfit * mfit, sizeof(double) * mfit);
     *chisq = back[(size_t)mfit * mfit + mfit];
     if (area_sum) *area_sum = back[(size_t)mfit * mfit + mfit + 1];
+    return PS_OK;
+}
+
+extern "C" ps_status ps_gpu_phase_clocks(ps_gpu *h, int32_t enable, int64_t *out)
+{
+    if (!h) return psb_fail(PS_ERR_NOT_PREPARED, "ps_gpu_phase_clocks: null handle");
+    PSB_CUDA(cudaSetDevice(h->device));
+    if (out) {
+        for (int i = 0; i < psb::kPhaseSlots; ++i) out[i] = 0;
+        if (h->phase.ptr) {
+            PSB_CUDA(cudaMemcpyAsync(out, h->phase.ptr, sizeof(int64_t) * psb::kPhaseSlots, cudaMemcpyDeviceToHost,
+                                     h->stream));
+            PSB_CUDA(cudaStreamSynchronize(h->stream));
+        }
+    }
+    if (enable) {
+        PSB_CUDA(h->phase.ensure(psb::kPhaseSlots));
+        PSB_CUDA(cudaMemsetAsync(h->phase.ptr, 0, sizeof(unsigned long long) * psb::kPhaseSlots, h->stream));
+        h->prm.phase_cycles = h->phase.ptr;
+    } else {
+        h->prm.phase_cycles = nullptr;
+        h->phase.release();
+    }
     return PS_OK;
 }
 

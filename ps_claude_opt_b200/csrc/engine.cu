@@ -21,12 +21,14 @@ int padded_ncoef(int n_coef)
     return -1;
 }
 
-size_t fit_smem_bytes(int n_fac, int mfit, int ncp) { return carve_bytes(n_fac, mfit, ncp, nullptr, nullptr); }
+size_t fit_smem_bytes(int n_fac, int mfit, int ncp, int n_curves, int row_stride, int tile_rows, int cstat_smem)
+{
+    return carve_bytes(n_fac, mfit, ncp, n_curves, row_stride, tile_rows, cstat_smem, nullptr, nullptr);
+}
 
 size_t fit_scratch_doubles(const DevObject &o)
 {
-    // derivative rows, per-curve statistics, point order + sort keys (2 ints per point)
-    size_t n = (size_t)o.n_points * o.row_stride + (size_t)o.n_curves * (o.ma + 3) + (size_t)o.n_points;
+    size_t n = scratch_perm(o.n_points, o.row_stride, o.n_curves, o.ma) + (size_t)o.n_points;
     return (n + 31) & ~size_t(31);
 }
 
@@ -52,7 +54,7 @@ static int prepare_kernel(const DevObject &o, KernelFn *fn, size_t *smem)
 {
     *fn = kernel_for(o.ncp);
     if (!*fn) return (int)cudaErrorInvalidValue;
-    *smem = fit_smem_bytes(o.n_fac, o.mfit, o.ncp);
+    *smem = fit_smem_bytes(o.n_fac, o.mfit, o.ncp, o.n_curves, o.row_stride, o.tile_rows, o.cstat_smem);
     cudaError_t e = cudaFuncSetAttribute(*fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
     return (int)e;
 }

@@ -20,11 +20,14 @@ constexpr int kMaxFac = 1024;
 
 struct DevObject {
     int n_points, n_curves, n_fac, n_coef, ncp, ma, mfit, row_stride;
+    int tile_rows;            // rows per J^T W J tile: 32, or 16 for the largest models
+    int cstat_smem;           // 1: per-curve statistics live in shared memory (they fit)
     const double4 *facet;     // [n_fac] {nx, ny, nz, d_area}
     const double *ysh;        // [n_fac][ncp] Laplace basis, zero-padded to ncp
     const double4 *pt_a;      // [n_points] {t, ee.x, ee.y, ee.z}
     const double4 *pt_b;      // [n_points] {ee0.x, ee0.y, ee0.z, brightness}
     const double *pt_w;       // [n_points] sigr2 * weight
+    const double4 *pt_rec;    // [n_points] {brightness, sigr2 * weight, curve index, relative flag}
     const int *pt_curve;      // [n_points] curve index
     const int *curve_start;   // [n_curves + 1]
     const int *curve_rel;     // [n_curves]
@@ -38,7 +41,11 @@ struct DevParams {
     double beta_pole[kPoles], lambda_pole[kPoles];
     double iter_diff_max, conw_r, conw_r_dev, freq_start, freq_step;
     int n_iter_max, n_iter_min;
+    // optional per-phase SM clock totals [kPhaseSlots] (nullptr: off)
+    unsigned long long *phase_cycles;
 };
+
+constexpr int kPhaseSlots = 12;  // 11 phases + evaluation count
 
 struct FitItem {
     int n_freq;   // 1-based frequency index
@@ -66,7 +73,7 @@ enum StatusBits : int {
 };
 
 // Bytes of dynamic shared memory one fit CTA needs.
-size_t fit_smem_bytes(int n_fac, int mfit, int ncp);
+size_t fit_smem_bytes(int n_fac, int mfit, int ncp, int n_curves, int row_stride, int tile_rows, int cstat_smem);
 // Doubles of scratch one CTA needs (derivative rows + per-curve statistics).
 size_t fit_scratch_doubles(const DevObject &o);
 // Padded coefficient count the kernels are compiled for.

@@ -28,7 +28,7 @@ namespace psb {
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kTiny = 1e-8;
 constexpr int kBPT = 5;  // 2x2 alpha blocks per thread: ceil(45*46/2 / 256)
-constexpr int kFacetChunk = 32;     // facets per shared-memory basis chunk
+constexpr int kStages = 4;          // basis chunks in flight in the facet sweep
 constexpr int kSortBands = 8;       // point sort: bands in cos(theta) ...
 constexpr int kSortSectors = 32;    // ... x sectors in longitude of the Sun-observer bisector
 constexpr int kSortCells = kSortBands * kSortSectors;
@@ -36,7 +36,17 @@ constexpr unsigned kWaitLimit = 1u << 24;  // bounded mbarrier waits
 
 // LM scalar slots in shared memory
 enum { S_ALAMDA, S_CHISQ, S_OCHISQ, S_ITERDIFF, S_DEVOLD, S_DEVNEW, S_CHCK, S_AREA, S_TRIAL, S_PIVINV, S_NSCAL };
-enum { C_ITEM, C_NITER, C_STATUS, C_ERR, C_IROW, C_ICOL, C_GO, C_ACCEPT, C_YUSE0, C_YUSE1, C_TIMEOUT, C_NCTL };
+enum { C_ITEM, C_NITER, C_STATUS, C_ERR, C_IROW, C_ICOL, C_GO, C_ACCEPT, C_TIMEOUT,
+       C_YUSE,                       // [kStages] completed uses of each chunk buffer
+       C_REL = C_YUSE + kStages,     // [kStages] warps done with the chunk in each buffer
+       C_TUSE = C_REL + kStages,     // [2] completed uses of each J^T W J tile buffer
+       C_NCTL = C_TUSE + 2 };
+// per-CTA phase clocks (optional instrumentation)
+enum { T_CURV, T_SORT, T_SWEEP, T_CSTAT, T_TILES, T_PSEUDO, T_SOLVE, T_REST, T_TWAIT, T_TSTAGE, T_TSYRK,
+       T_NPHASE };
+
+// Facets per basis chunk: keeps kStages chunks within ~60 KB of shared memory.
+__host__ __device__ inline int chunk_facets(int ncp) { return ncp <= 64 ? 32 : 16; }
 
 struct Sh {
     double4 *F;       // [n_fac] normal + current area
@@ -46,13 +56,24 @@ struct Sh {
     double *da;       // [kMaxFit]
     double *a;        // [kMaxPar]
     double *atry;     // [kMaxPar]
-    double *T;        // [kTile][mfp]       (shares storage with ybuf)
-    double *TW;       // [kTile][mfp]       (shares storage with ybuf)
-    double *ybuf;     // [2][kFacetChunk][ncp] basis chunks of the facet sweep
-    unsigned long long *mbar;  // [2] completion barriers of the chunk copies
+    double *T;        // [tile_rows][mfp]       (shares storage with ybuf)
+    double *TW;       // [tile_rows][mfp]       (shares storage with ybuf)
+    double *raw;      // [2][tile_rows][row_stride] raw rows of the tile (shares with ybuf)
+    double4 *recb;    // [2][tile_rows] per-point records of the tile (shares with ybuf)
+    unsigned long long *tbar;  // [2] completion barriers of the tile copies
+    double *ccoef;    // [n_curves] renormalisation coefficient of each relative curve
+    double *crave;    // [n_curves] 1 / sum(ymod) of each relative curve
+    double *cst;      // [n_curves][ma + 3] per-curve statistics (when they fit here)
+    double *wst;      // [kWarps][32][4] facet weights of one k-step, per warp (sweep MMA operand A)
+    double *ybuf;     // [kStages][chunk_facets][ncp] basis chunks of the facet sweep
+    unsigned long long *mbar;  // [kStages] completion barriers of the chunk copies
+    long long *tclk;  // [T_NPHASE + 1] phase clocks, last slot = previous mark
     int *hist;        // [2][kSortCells] point-sort histogram and offsets
-    double *rdy;      // [kTile]
-    double *rw;       // [kTile]
+    double *rdy;      // [kTile] per-row residual y - ymod
+    double *rw;       // [kTile] per-row weight sigr2 * weight
+    double *rcoef;    // [kTile] per-row renormalisation coefficient (relative curves)
+    double *rsub;     // [kTile] per-row ymod * rave (relative curves)
+    int *rcur;        // [kTile] per-row curve index if relative, else -1
     double *red;      // [kWarps * 4]
     double *inv;      // [40] per-evaluation invariants
     double *scal;     // [S_NSCAL]
@@ -60,7 +81,7 @@ struct Sh {
     int *fidx;        // [kMaxFit]
     int *ipiv;        // [kMaxFit]
     int *ctl;         // [C_NCTL]
-    int ld, mfp;
+    int ld, mfp, tr;
 };
 
 __device__ __forceinline__ double4 ldg4(const double4 *p)
@@ -112,12 +133,46 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t pari
     return false;
 }
 
+// Charges the cycles since the previous mark to `phase` (thread 0, when the
+// caller asked for phase clocks).
+__device__ __forceinline__ void tmark(const DevParams &p, const Sh &s, int phase)
+{
+    if (p.phase_cycles && threadIdx.x == 0) {
+        const long long now = clock64();
+        s.tclk[phase] += now - s.tclk[T_NPHASE];
+        s.tclk[T_NPHASE] = now;
+    }
+}
+
 __host__ __device__ inline int fit_ld(int mfit) { return mfit | 1; }
-__host__ __device__ inline int fit_mfp(int mfit) { return (mfit + 1) & ~1; }
+// Row stride of the J^T W J staging tiles: the augmented width mfit + 1
+// rounded to whole 8-column MMA blocks, then to 4 mod 16 doubles so the
+// 8x4 / 4x8 fragment loads of a half-warp hit 16 distinct 8-byte banks.
+__host__ __device__ inline int fit_mpad(int mfit) { return (mfit + 1 + 7) & ~7; }
+__host__ __device__ inline int fit_mfp(int mfit)
+{
+    const int mp = fit_mpad(mfit);
+    return mp + ((4 - mp) & 15);
+}
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-__host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, Sh *s, unsigned char *base)
+// Scratch slab of one CTA, in doubles from its start:
+//   [0, n_points * row_stride)             derivative rows
+//   [.., + n_curves * (ma + 3))            per-curve statistics
+//   [gpart, + kWarps * 36 * 64)            rank-k partial sums (16-byte aligned)
+//   [perm, + n_points)                     point order and sort keys (2 ints each)
+__host__ __device__ inline size_t scratch_gpart(int n_points, int row_stride, int n_curves, int ma)
+{
+    return ((size_t)n_points * row_stride + (size_t)n_curves * (ma + 3) + 1) & ~size_t(1);
+}
+__host__ __device__ inline size_t scratch_perm(int n_points, int row_stride, int n_curves, int ma)
+{
+    return scratch_gpart(n_points, row_stride, n_curves, ma) + (size_t)kWarps * 36 * 64;
+}
+
+__host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, int n_curves, int rs, int tr,
+                                              int cstat_smem, Sh *s, unsigned char *base)
 {
     int ld = fit_ld(mfit), mfp = fit_mfp(mfit);
     size_t off = 0;
@@ -133,18 +188,19 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, Sh *
     void *da = take(sizeof(double) * kMaxFit);
     void *a = take(sizeof(double) * kMaxPar);
     void *atry = take(sizeof(double) * kMaxPar);
-    // the JtWJ tiles (phase D) and the basis chunks (phase B) are never live
-    // at the same time: one region serves both
-    const size_t tiles = 2 * align16(sizeof(double) * kTile * mfp);
-    const size_t chunks = 2 * sizeof(double) * kFacetChunk * ncp;
+    // the J^T W J tile buffers (phase D) and the basis chunks (phase B) are
+    // never live at the same time: one region serves both
+    const size_t tsz = align16(sizeof(double) * tr * mfp);
+    const size_t rsz = align16(sizeof(double) * tr * rs);
+    const size_t csz = align16(sizeof(double4) * tr);
+    const size_t tiles = 2 * tsz + 2 * rsz + 2 * csz;
+    const size_t chunks = (size_t)kStages * sizeof(double) * chunk_facets(ncp) * ncp;
     unsigned char *un = (unsigned char *)take(tiles > chunks ? tiles : chunks);
-    void *T = un;
-    void *TW = un ? un + align16(sizeof(double) * kTile * mfp) : nullptr;
-    void *ybuf = un;
-    void *mbar = take(sizeof(unsigned long long) * 2);
-    void *hist = take(sizeof(int) * 2 * kSortCells);
     void *rdy = take(sizeof(double) * kTile);
     void *rw = take(sizeof(double) * kTile);
+    void *rcoef = take(sizeof(double) * kTile);
+    void *rsub = take(sizeof(double) * kTile);
+    void *rcur = take(sizeof(int) * kTile);
     void *red = take(sizeof(double) * kWarps * 4);
     void *inv = take(sizeof(double) * 40);
     void *scal = take(sizeof(double) * S_NSCAL);
@@ -152,14 +208,32 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, Sh *
     void *fidx = take(sizeof(int) * kMaxFit);
     void *ipiv = take(sizeof(int) * kMaxFit);
     void *ctl = take(sizeof(int) * C_NCTL);
+    void *mbar = take(sizeof(unsigned long long) * kStages);
+    void *tbar = take(sizeof(unsigned long long) * 2);
+    void *tclk = take(sizeof(long long) * (T_NPHASE + 1));
+    void *hist = take(sizeof(int) * 2 * kSortCells);
+    void *ccoef = take(sizeof(double) * n_curves);
+    void *crave = take(sizeof(double) * n_curves);
+    // rs = row stride = ma + 1 rounded to even, so ma + 3 <= rs + 2
+    void *cst = take(cstat_smem ? sizeof(double) * n_curves * (rs + 2) : 0);
+    void *wst = take(sizeof(double) * kWarps * 32 * 4);
     if (s) {
         s->F = (double4 *)F; s->alpha = (double *)alpha; s->covar = (double *)covar;
         s->beta = (double *)beta; s->da = (double *)da; s->a = (double *)a; s->atry = (double *)atry;
-        s->T = (double *)T; s->TW = (double *)TW; s->rdy = (double *)rdy; s->rw = (double *)rw;
-        s->ybuf = (double *)ybuf; s->mbar = (unsigned long long *)mbar; s->hist = (int *)hist;
+        s->T = (double *)un;
+        s->TW = (double *)(un + tsz);
+        s->raw = (double *)(un + 2 * tsz);
+        s->recb = (double4 *)(un + 2 * tsz + 2 * rsz);
+        s->ybuf = (double *)un;
+        s->rdy = (double *)rdy; s->rw = (double *)rw;
+        s->rcoef = (double *)rcoef; s->rsub = (double *)rsub; s->rcur = (int *)rcur;
         s->red = (double *)red; s->inv = (double *)inv; s->scal = (double *)scal;
         s->colbuf = (double *)colbuf; s->fidx = (int *)fidx; s->ipiv = (int *)ipiv; s->ctl = (int *)ctl;
-        s->ld = ld; s->mfp = mfp;
+        s->mbar = (unsigned long long *)mbar; s->tbar = (unsigned long long *)tbar;
+        s->tclk = (long long *)tclk; s->hist = (int *)hist;
+        s->ccoef = (double *)ccoef; s->crave = (double *)crave; s->cst = (double *)cst;
+        s->wst = (double *)wst;
+        s->ld = ld; s->mfp = mfp; s->tr = tr;
     }
     return off;
 }
@@ -378,33 +452,52 @@ static __device__ void sort_points(const DevObject &o, const Sh &s, int *perm, i
 // (Start.cu:2262-2535).  Row layout: column p-1 = d ymod / d a_p for
 // p = 1..ma, column ma = ymod (un-renormalised).
 //
-// All warps sweep the facets in lockstep, kFacetChunk facets at a time; the
-// chunk's basis rows (ncp doubles each) arrive in shared memory by bulk copy,
-// double-buffered, so the shape-derivative loop reads broadcast shared-memory
-// operands.  One warp = 32 points (lane = point), shape-derivative sums in
-// registers.
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// The facet sweep is a kStages-deep pipeline of basis chunks (chunk_facets
+// facets x ncp doubles each) that the bulk-copy engine brings into shared
+// memory.  Every warp walks the same chunk sequence; the last warp to finish
+// with a buffer issues the copy of the chunk kStages ahead into it, so warps
+// drift apart by up to kStages - 1 chunks instead of meeting at a CTA barrier
+// per chunk.
+//
+// One warp = 32 points.  Per facet, lane = point computes visibility, the
+// Lambert + Lommel-Seeliger terms and the rotation-derivative sums; whole
+// facets no lane sees are skipped.  The shape derivatives
+//     J[p][k] = sum_f w[p][f] Y[f][k],   w[p][f] = Areag_f s(mu, mu0)
+// are a GEMM: each group of 4 facets is one k-step of FP64 tensor-core
+// MMAs (m8n8k4), A = w (8 points x 4 facets, staged through a per-warp
+// shared-memory tile), B = the basis chunk (4 facets x 8 coefficients),
+// accumulators [4 point blocks][ncp / 8 coefficient blocks] in registers.
 template <int NCP>
 __device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows, const int *perm)
 {
+    constexpr int NT = NCP / 8;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int np = o.n_points, nf = o.n_fac, nc = o.n_coef, RS = o.row_stride;
+    const int np = o.n_points, nf = o.n_fac, nc = o.n_coef;
     const double cl = s.inv[5], cls = s.inv[6];
-    const int nchunks = (nf + kFacetChunk - 1) / kFacetChunk;
+    const int fc = chunk_facets(NCP);
+    const int nchunks = (nf + fc - 1) / fc;
     const int ntiles = (np + 31) / 32;
     const int nrounds = (ntiles + kWarps - 1) / kWarps;
     const int total = nrounds * nchunks;
-    int use[2] = {s.ctl[C_YUSE0], s.ctl[C_YUSE1]};  // completed waits per buffer (parity source)
+    double *wt = s.wst + warp * 32 * 4;
     bool timeout = false;
 
     auto issue = [&](int g) {
-        const int c = g % nchunks, f0 = c * kFacetChunk;
-        const int rows_c = min(kFacetChunk, nf - f0);
-        const int b = g & 1;
-        bulk_load(s.ybuf + (size_t)b * kFacetChunk * NCP, o.ysh + (size_t)f0 * NCP,
+        const int c = g % nchunks, f0 = c * fc;
+        const int rows_c = min(fc, nf - f0);
+        const int b = g % kStages;
+        bulk_load(s.ybuf + (size_t)b * fc * NCP, o.ysh + (size_t)f0 * NCP,
                   (uint32_t)(rows_c * NCP * sizeof(double)), &s.mbar[b]);
     };
     if (tid == 0)
-        for (int g = 0; g < 2 && g < total; ++g) issue(g);
+        for (int g = 0; g < kStages && g < total; ++g) issue(g);
 
     int g = 0;
     for (int round = 0; round < nrounds; ++round) {
@@ -413,86 +506,116 @@ __device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows, c
         const int idx = tile * 32 + lane;
         const bool act = tile_act && idx < np;
         const int p = perm[min(idx, np - 1)];
-        double t = 0, ee[3] = {0, 0, 0}, es[3] = {0, 0, 0};
+        double ex, ey, ez, sx, sy, sz;
         {
             const double4 pa = ldg4(&o.pt_a[p]);
             const double4 pb = ldg4(&o.pt_b[p]);
-            t = pa.x;
-            ee[0] = pa.y; ee[1] = pa.z; ee[2] = pa.w;
-            es[0] = pb.x; es[1] = pb.y; es[2] = pb.z;
+            const double ee[3] = {pa.y, pa.z, pa.w}, es[3] = {pb.x, pb.y, pb.z};
+            PointGeo geo;
+            point_geometry<false>(s.inv, pa.x, ee, es, geo);
+            ex = geo.e[0]; ey = geo.e[1]; ez = geo.e[2];
+            sx = geo.e0[0]; sy = geo.e0[1]; sz = geo.e0[2];
         }
-        PointGeo geo;
-        point_geometry<false>(s.inv, t, ee, es, geo);
-        const double ex = geo.e[0], ey = geo.e[1], ez = geo.e[2];
-        const double sx = geo.e0[0], sy = geo.e0[1], sz = geo.e0[2];
 
-        double J[NCP];
+        double C[4][NT][2];
 #pragma unroll
-        for (int k = 0; k < NCP; ++k) J[k] = 0.0;
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+            for (int n = 0; n < NT; ++n) C[m][n][0] = C[m][n][1] = 0.0;
         double br = 0, u0 = 0, u1 = 0, u2 = 0, w0 = 0, w1 = 0, w2 = 0, t4 = 0, t5 = 0;
 
         for (int c = 0; c < nchunks; ++c, ++g) {
-            const int b = g & 1;
-            if (!mbar_wait(&s.mbar[b], (uint32_t)(use[b] & 1))) timeout = true;
+            const int b = g % kStages;
+            const int use = s.ctl[C_YUSE + b] + g / kStages;  // phase parity of this fill
+            if (!mbar_wait(&s.mbar[b], (uint32_t)(use & 1))) timeout = true;
             if (tile_act) {
-                const int f0 = c * kFacetChunk, f1 = min(nf, f0 + kFacetChunk);
-                const double *yb = s.ybuf + (size_t)b * kFacetChunk * NCP;
+                const int f0 = c * fc, nfc = min(fc, nf - f0);
+                const double *yb = s.ybuf + (size_t)b * fc * NCP;
 #pragma unroll 1
-                for (int fi = f0; fi < f1; ++fi) {
-                    const double4 fr = s.F[fi];
-                    const double mu = ex * fr.x + ey * fr.y + ez * fr.z;
-                    const double mu0 = sx * fr.x + sy * fr.y + sz * fr.z;
-                    const bool vis = act && (mu > kTiny) && (mu0 > kTiny);
-                    if (__any_sync(0xffffffffu, vis)) {
-                        // lanes that do not see the facet run the same arithmetic on
-                        // finite stand-ins and contribute exact zeros
-                        const double ar = vis ? fr.w : 0.0;
-                        const double r = __drcp_rn(vis ? mu + mu0 : 1.0);
-                        const double sv = mu * mu0 * (cl + cls * r);
-                        const double q0 = mu0 * r, q1 = mu * r;
-                        const double dsmu = cls * (q0 * q0) + cl * mu0;
-                        const double dsmu0 = cls * (q1 * q1) + cl * mu;
-                        const double amm = ar * mu * mu0;
-                        const double w = ar * sv;
-                        const double gg = ar * dsmu;
-                        const double g0 = ar * dsmu0;
-                        br += w;
-                        u0 = fma(gg, fr.x, u0);
-                        u1 = fma(gg, fr.y, u1);
-                        u2 = fma(gg, fr.z, u2);
-                        w0 = fma(g0, fr.x, w0);
-                        w1 = fma(g0, fr.y, w1);
-                        w2 = fma(g0, fr.z, w2);
-                        t4 += amm;
-                        t5 += amm * r;
-                        const double2 *yr = reinterpret_cast<const double2 *>(yb + (size_t)(fi - f0) * NCP);
+                for (int k0 = 0; k0 < nfc; k0 += 4) {
+                    double wk[4];
+                    bool any4 = false;
 #pragma unroll
-                        for (int k = 0; k < NCP / 2; ++k) {
-                            const double2 y = yr[k];
-                            J[2 * k] = fma(w, y.x, J[2 * k]);
-                            J[2 * k + 1] = fma(w, y.y, J[2 * k + 1]);
+                    for (int q = 0; q < 4; ++q) {
+                        wk[q] = 0.0;
+                        if (k0 + q < nfc) {
+                            const double4 fr = s.F[f0 + k0 + q];
+                            const double mu = ex * fr.x + ey * fr.y + ez * fr.z;
+                            const double mu0 = sx * fr.x + sy * fr.y + sz * fr.z;
+                            const bool vis = act && (mu > kTiny) && (mu0 > kTiny);
+                            if (__any_sync(0xffffffffu, vis)) {
+                                // lanes that do not see the facet run the same arithmetic on
+                                // finite stand-ins and contribute exact zeros
+                                const double ar = vis ? fr.w : 0.0;
+                                const double r = __drcp_rn(vis ? mu + mu0 : 1.0);
+                                const double sv = mu * mu0 * (cl + cls * r);
+                                const double q0 = mu0 * r, q1 = mu * r;
+                                const double dsmu = cls * (q0 * q0) + cl * mu0;
+                                const double dsmu0 = cls * (q1 * q1) + cl * mu;
+                                const double amm = ar * mu * mu0;
+                                const double w = ar * sv;
+                                const double gg = ar * dsmu;
+                                const double g0 = ar * dsmu0;
+                                br += w;
+                                u0 = fma(gg, fr.x, u0);
+                                u1 = fma(gg, fr.y, u1);
+                                u2 = fma(gg, fr.z, u2);
+                                w0 = fma(g0, fr.x, w0);
+                                w1 = fma(g0, fr.y, w1);
+                                w2 = fma(g0, fr.z, w2);
+                                t4 += amm;
+                                t5 += amm * r;
+                                wk[q] = w;
+                                any4 = true;
+                            }
                         }
+                    }
+                    if (any4) {  // warp-uniform
+                        reinterpret_cast<double2 *>(wt)[2 * lane] = make_double2(wk[0], wk[1]);
+                        reinterpret_cast<double2 *>(wt)[2 * lane + 1] = make_double2(wk[2], wk[3]);
+                        __syncwarp();
+                        double a[4];
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) a[m] = wt[(8 * m + (lane >> 2)) * 4 + (lane & 3)];
+                        // B row = facet k0 + (lane & 3); rows past the chunk's end hold
+                        // stale data and must contribute zeros
+                        const bool brow = k0 + (lane & 3) < nfc;
+                        const double *yr = yb + (size_t)(k0 + (lane & 3)) * NCP + (lane >> 2);
+#pragma unroll
+                        for (int n = 0; n < NT; ++n) {
+                            const double bv = brow ? yr[8 * n] : 0.0;
+#pragma unroll
+                            for (int m = 0; m < 4; ++m) dmma_8x8x4(C[m][n][0], C[m][n][1], a[m], bv);
+                        }
+                        __syncwarp();
                     }
                 }
             }
-            __syncthreads();  // every warp is done with buffer b
-            use[b] += 1;
-            if (tid == 0 && g + 2 < total) issue(g + 2);
+            // release the buffer; the last of the kWarps warps refills it
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                if (atomicAdd(&s.ctl[C_REL + b], 1) == kWarps - 1) {
+                    s.ctl[C_REL + b] = 0;
+                    if (g + kStages < total) issue(g + kStages);
+                }
+            }
         }
 
         if (tile_act) {
-            point_geometry<true>(s.inv, t, ee, es, geo);
+            const double4 pa = ldg4(&o.pt_a[p]);
+            const double4 pb = ldg4(&o.pt_b[p]);
+            const double ee[3] = {pa.y, pa.z, pa.w}, es[3] = {pb.x, pb.y, pb.z};
+            PointGeo geo;
+            point_geometry<true>(s.inv, pa.x, ee, es, geo);
             const double t1 = (geo.db[0] * u0 + geo.db[1] * u1 + geo.db[2] * u2) +
                               (geo.d0b[0] * w0 + geo.d0b[1] * w1 + geo.d0b[2] * w2);
             const double t2 = (geo.dl[0] * u0 + geo.dl[1] * u1 + geo.dl[2] * u2) +
                               (geo.d0l[0] * w0 + geo.d0l[1] * w1 + geo.d0l[2] * w2);
             const double t3 = (geo.dw[0] * u0 + geo.dw[1] * u1) + (geo.d0w[0] * w0 + geo.d0w[1] * w1);
+            const double scale = geo.scale;
             if (act) {
-                const double scale = geo.scale;
-                double *row = rows + (size_t)p * RS;
-#pragma unroll
-                for (int k = 0; k < NCP; ++k)
-                    if (k < nc) row[k] = scale * J[k];
+                double *row = rows + (size_t)p * o.row_stride;
                 row[nc + 0] = scale * t1;
                 row[nc + 1] = scale * t2;
                 row[nc + 2] = scale * t3;
@@ -503,71 +626,181 @@ __device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows, c
                 row[nc + 7] = scale * t5;
                 row[nc + 8] = br * scale;
             }
+            // shape columns from the MMA accumulators: element (m, n, e) of this
+            // lane is point 8m + lane/4 of the tile, coefficient 8n + 2(lane%4) + e
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int src = 8 * m + (lane >> 2);
+                const int pm = __shfl_sync(0xffffffffu, p, src);
+                const double sm = __shfl_sync(0xffffffffu, scale, src);
+                const bool am = __shfl_sync(0xffffffffu, act ? 1 : 0, src) != 0;
+                if (!am) continue;
+                double *row = rows + (size_t)pm * o.row_stride;
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    const int k = 8 * n + 2 * (lane & 3);
+                    if (k + 1 < nc)
+                        *reinterpret_cast<double2 *>(row + k) = make_double2(sm * C[m][n][0], sm * C[m][n][1]);
+                    else if (k < nc)
+                        row[k] = sm * C[m][n][0];
+                }
+            }
         }
     }
     if (timeout) s.ctl[C_TIMEOUT] = 1;
+    __syncthreads();
+    // per-buffer fill counts carry the mbarrier phases into the next evaluation
     if (tid == 0) {
-        s.ctl[C_YUSE0] = use[0];
-        s.ctl[C_YUSE1] = use[1];
+        for (int b = 0; b < kStages; ++b) {
+            const int uses_b = (total > b) ? (total - b + kStages - 1) / kStages : 0;
+            s.ctl[C_YUSE + b] += uses_b;
+        }
     }
 }
 
 // ---------------------------------------------------------------- phases C, D
 
-struct AlphaAcc {
-    double v[kBPT][4];
-    int bj[kBPT], bk[kBPT];
-    int nb;
+// J^T W J, J^T W dy and chi^2 as one symmetric rank-k update of the augmented
+// matrix [J | dy] on the FP64 tensor cores (mma.sync m8n8k4 .f64):
+//   C = A B,  A[j][r] = TW[r][j] = J[r][j] w_r,  B[r][k] = T[r][k] = J[r][k],
+// with column mfit of T holding dy_r and of TW holding dy_r w_r, so
+//   C[j][k] = alpha_jk,  C[mfit][k] = beta_k,  C[mfit][mfit] = chi^2.
+// Only lower-triangle 8x8 blocks are computed; warps own blocks round-robin
+// and keep their accumulators in registers for the whole evaluation.
+constexpr int kSliceBlk = 36;  // k-slice mode: all 8 x 9 / 2 lower blocks of a <= 64-wide matrix
+constexpr int kMaxBlk = 10;    // block mode: ceil(78 / 8) blocks per warp for <= 96-wide matrices
+
+// Two ways to spread the augmented rank-k update over the 8 warps:
+//  * k-slice mode (<= 8 x 8 blocks): warp w takes rows 4w..4w+3 of every tile
+//    and updates every lower block with them, so each A / B fragment is
+//    loaded once per k-step and reused by up to 8 MMAs; the 8 partial sums
+//    are added in warp order at the end.
+//  * block mode (larger models): warps own blocks round-robin over all rows.
+struct SyrkAcc {
+    double c[kSliceBlk][2];
+    int nb;       // blocks per dimension
+    int slice;    // 1: k-slice mode
+    int bj[kMaxBlk], bk[kMaxBlk], nblk;   // block mode
 };
 
-__device__ __forceinline__ void alpha_blocks(int mfit, AlphaAcc &acc)
+__device__ __forceinline__ void syrk_init(int mfit, int tile_rows, SyrkAcc &acc)
 {
-    const int nb = (mfit + 1) / 2;
-    const int nblocks = nb * (nb + 1) / 2;
-    acc.nb = 0;
+    const int warp = threadIdx.x >> 5;
+    acc.nb = fit_mpad(mfit) / 8;
+    acc.slice = (acc.nb <= 8 && tile_rows == 4 * kWarps) ? 1 : 0;
+    const int nblocks = acc.nb * (acc.nb + 1) / 2;
+    acc.nblk = 0;
 #pragma unroll
-    for (int i = 0; i < kBPT; ++i) {
-        int b = threadIdx.x + i * kThreads;
-        int bj = 0, bk = 0;
-        if (b < nblocks) {
-            bj = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
-            while ((bj + 1) * (bj + 2) / 2 <= b) ++bj;
-            while (bj * (bj + 1) / 2 > b) --bj;
-            bk = b - bj * (bj + 1) / 2;
-            acc.nb = i + 1;
-        }
+    for (int i = 0; i < kMaxBlk; ++i) {
+        const int b = warp + i * kWarps;
+        int bj = 0;
+        while ((bj + 1) * (bj + 2) / 2 <= b) ++bj;
         acc.bj[i] = bj;
-        acc.bk[i] = bk;
+        acc.bk[i] = b - bj * (bj + 1) / 2;
+        if (b < nblocks) acc.nblk = i + 1;
+    }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc.v[i][q] = 0.0;
+    for (int i = 0; i < kSliceBlk; ++i) acc.c[i][0] = acc.c[i][1] = 0.0;
+}
+
+// Accumulates one staged tile (rows 0..nrows-1 of T/TW, zero beyond).
+__device__ __forceinline__ void syrk_update(const Sh &s, int nrows, SyrkAcc &acc)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int S = s.mfp;
+    const int kq = lane & 3, cq = lane >> 2;
+    if (acc.slice) {
+        const int r0 = 4 * warp;
+        if (r0 >= nrows) return;
+        const double *tw = s.TW + (r0 + kq) * S + cq;
+        const double *tt = s.T + (r0 + kq) * S + cq;
+        double a[8], b[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            a[q] = (q < acc.nb) ? tw[8 * q] : 0.0;
+            b[q] = (q < acc.nb) ? tt[8 * q] : 0.0;
+        }
+#pragma unroll
+        for (int bj = 0; bj < 8; ++bj)
+#pragma unroll
+            for (int bk = 0; bk <= bj; ++bk)
+                if (bj < acc.nb) {
+                    const int i = bj * (bj + 1) / 2 + bk;
+                    dmma_8x8x4(acc.c[i][0], acc.c[i][1], a[bj], b[bk]);
+                }
+        return;
+    }
+    for (int r0 = 0; r0 < nrows; r0 += 4) {
+        const double *tw = s.TW + (r0 + kq) * S + cq;
+        const double *tt = s.T + (r0 + kq) * S + cq;
+#pragma unroll
+        for (int i = 0; i < kMaxBlk; ++i)
+            if (i < acc.nblk) dmma_8x8x4(acc.c[i][0], acc.c[i][1], tw[8 * acc.bj[i]], tt[8 * acc.bk[i]]);
     }
 }
 
-// Accumulates one staged tile of nrows rows into alpha, beta and chi^2.
-__device__ __forceinline__ void tile_update(const Sh &s, int mfit, int nrows, AlphaAcc &acc,
-                                            double &beta_j, double &chisq)
+// Adds one warp's accumulators into alpha (lower triangle mirrored, stride
+// ld), beta and chi^2.
+__device__ __forceinline__ void syrk_add_block(const Sh &s, int mfit, int bj, int bk, double v0, double v1,
+                                               double *dst, double *dvec, bool first)
 {
-    const int mfp = s.mfp;
+    const int lane = threadIdx.x & 31, ld = s.ld;
 #pragma unroll
-    for (int i = 0; i < kBPT; ++i) {
-        if (i < acc.nb) {
-            const int j0 = 2 * acc.bj[i], k0 = 2 * acc.bk[i];
-            double a00 = acc.v[i][0], a01 = acc.v[i][1], a10 = acc.v[i][2], a11 = acc.v[i][3];
-            for (int rr = 0; rr < nrows; ++rr) {
-                const double2 tw = *reinterpret_cast<const double2 *>(s.TW + rr * mfp + j0);
-                const double2 tt = *reinterpret_cast<const double2 *>(s.T + rr * mfp + k0);
-                a00 = fma(tw.x, tt.x, a00);
-                a01 = fma(tw.x, tt.y, a01);
-                a10 = fma(tw.y, tt.x, a10);
-                a11 = fma(tw.y, tt.y, a11);
-            }
-            acc.v[i][0] = a00; acc.v[i][1] = a01; acc.v[i][2] = a10; acc.v[i][3] = a11;
+    for (int e = 0; e < 2; ++e) {
+        const int row = 8 * bj + (lane >> 2);
+        const int col = 8 * bk + 2 * (lane & 3) + e;
+        const double v = e ? v1 : v0;
+        if (row < mfit && col <= row) {
+            const double t = first ? v : dst[row * ld + col] + v;
+            dst[row * ld + col] = t;
+            if (col != row) dst[col * ld + row] = t;
+        } else if (row == mfit && col < mfit) {
+            dvec[col] = first ? v : dvec[col] + v;
+        } else if (row == mfit && col == mfit) {
+            s.scal[S_TRIAL] = first ? v : s.scal[S_TRIAL] + v;
         }
     }
-    if (threadIdx.x < mfit)
-        for (int rr = 0; rr < nrows; ++rr) beta_j = fma(s.rdy[rr], s.TW[rr * mfp + threadIdx.x], beta_j);
-    if (threadIdx.x == 0)
-        for (int rr = 0; rr < nrows; ++rr) chisq = fma(s.rdy[rr] * s.rdy[rr], s.rw[rr], chisq);
+}
+
+// Writes the accumulated alpha, beta and chi^2 (all threads call this).  In
+// k-slice mode the 8 warps' partial sums go through a scratch slab (L2) and
+// are added in warp order, element by element, by all threads.
+__device__ __forceinline__ void syrk_store(const Sh &s, int mfit, const SyrkAcc &acc, double *dst, double *dvec,
+                                           double *gpart)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (acc.slice) {
+        const int nblocks = acc.nb * (acc.nb + 1) / 2;
+        double2 *mine = reinterpret_cast<double2 *>(gpart) + (size_t)warp * kSliceBlk * 32;
+#pragma unroll
+        for (int i = 0; i < kSliceBlk; ++i)
+            if (i < nblocks) mine[i * 32 + lane] = make_double2(acc.c[i][0], acc.c[i][1]);
+        __syncthreads();
+        const int ld = s.ld;
+        for (int idx = tid; idx < nblocks * 64; idx += kThreads) {
+            const int i = idx >> 6, l = (idx >> 1) & 31, e = idx & 1;
+            double v = 0.0;
+            for (int w = 0; w < kWarps; ++w) v += gpart[((size_t)w * kSliceBlk * 32 + i * 32 + l) * 2 + e];
+            int bj = 0;
+            while ((bj + 1) * (bj + 2) / 2 <= i) ++bj;
+            const int bk = i - bj * (bj + 1) / 2;
+            const int row = 8 * bj + (l >> 2), col = 8 * bk + 2 * (l & 3) + e;
+            if (row < mfit && col <= row) {
+                dst[row * ld + col] = v;
+                dst[col * ld + row] = v;
+            } else if (row == mfit && col < mfit) {
+                dvec[col] = v;
+            } else if (row == mfit && col == mfit) {
+                s.scal[S_TRIAL] = v;
+            }
+        }
+        __syncthreads();
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < kMaxBlk; ++i)
+        if (i < acc.nblk) syrk_add_block(s, mfit, acc.bj[i], acc.bk[i], acc.c[i][0], acc.c[i][1], dst, dvec, true);
+    __syncthreads();
 }
 
 // One full evaluation (mrqcof) at parameter vector a in shared memory.
@@ -580,13 +813,20 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ma = o.ma, mfit = o.mfit, mfp = s.mfp, RS = o.row_stride, CS = ma + 3;
 
+    if (o.cstat_smem) cstat = s.cst;  // stride ma + 3 fits inside rs + 2
+    tmark(p, s, T_REST);
     double area_sum = shape_areas(o, s, a);
     if (tid == 0) s.scal[S_AREA] = area_sum;
     set_invariants(o, p, s, a);
+    tmark(p, s, T_CURV);
 
     sort_points(o, s, perm, perm + o.n_points);
+    tmark(p, s, T_SORT);
     brightness_rows<NCP>(o, s, rows, perm);
+    // the tile phase reads the rows back through the bulk-copy (async) proxy
+    asm volatile("fence.proxy.async.global;" ::: "memory");
     __syncthreads();
+    tmark(p, s, T_SWEEP);
 
     // per relative curve: column sums, 1/sum(ymod) and the renormalisation coefficient
     for (int c = warp; c < o.n_curves; c += kWarps) {
@@ -599,57 +839,109 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
         }
         __syncwarp();
         if (lane == 0) {
-            double rave = 1.0 / cstat[(size_t)c * CS + ma];
+            const double rave = 1.0 / cstat[(size_t)c * CS + ma];
+            const double coef = o.curve_sig[c] * (p1 - p0) * rave;
             cstat[(size_t)c * CS + ma + 1] = rave;
-            cstat[(size_t)c * CS + ma + 2] = o.curve_sig[c] * (p1 - p0) * rave;
+            cstat[(size_t)c * CS + ma + 2] = coef;
+            s.crave[c] = rave;
+            s.ccoef[c] = coef;
         }
     }
     __syncthreads();
+    tmark(p, s, T_CSTAT);
 
-    AlphaAcc acc;
-    alpha_blocks(mfit, acc);
-    double beta_j = 0.0, chisq = 0.0;
+    SyrkAcc acc;
+    syrk_init(mfit, s.tr, acc);
 
-    const int np = o.n_points;
-    for (int r0 = 0; r0 < np; r0 += kTile) {
-        const int nrows = min(kTile, np - r0);
-        for (int idx = tid; idx < kTile * mfp; idx += kThreads) {
-            const int rr = idx / mfp, j = idx - rr * mfp;
-            const int q = r0 + rr;
-            double v = 0.0, vw = 0.0;
-            if (rr < nrows && j < mfit) {
-                const int col = s.fidx[j] - 1;
-                const double raw = rows[(size_t)q * RS + col];
-                const int c = __ldg(&o.pt_curve[q]);
-                if (__ldg(&o.curve_rel[c])) {
-                    const double *cs = cstat + (size_t)c * CS;
-                    const double coef1 = rows[(size_t)q * RS + ma] * cs[ma + 1];
-                    v = cs[ma + 2] * (raw - coef1 * cs[col]);
-                } else {
-                    v = raw;
-                }
-                vw = v * __ldg(&o.pt_w[q]);
-            }
-            s.T[idx] = v;
-            s.TW[idx] = vw;
-        }
-        if (tid < kTile) {
-            double dy = 0.0, w = 0.0;
-            if (tid < nrows) {
-                const int q = r0 + tid;
-                const int c = __ldg(&o.pt_curve[q]);
-                double ymod = rows[(size_t)q * RS + ma];
-                if (__ldg(&o.curve_rel[c])) ymod = cstat[(size_t)c * CS + ma + 2] * ymod;
-                dy = __ldg(&o.pt_b[q].w) - ymod;
-                w = __ldg(&o.pt_w[q]);
-            }
-            s.rdy[tid] = dy;
-            s.rw[tid] = w;
-        }
-        __syncthreads();
-        tile_update(s, mfit, nrows, acc, beta_j, chisq);
-        __syncthreads();
+    // J^T W J tiles: the raw rows of tile t (tile_rows consecutive points)
+    // and their per-point records arrive by bulk copy, double-buffered, while
+    // the tensor cores work on tile t - 1.  Each warp stages tile_rows / 8
+    // rows: renormalisation (relative curves, Start.cu:2660-2693) and
+    // compaction to the fitted parameters.
+    const int np = o.n_points, TR = s.tr, rpw = TR / kWarps;
+    const int ntile = (np + TR - 1) / TR;
+    auto tissue = [&](int t) {
+        const int r0 = t * TR, nr = min(TR, np - r0), b = t & 1;
+        bulk_load(s.raw + (size_t)b * TR * RS, rows + (size_t)r0 * RS, (uint32_t)(nr * RS * sizeof(double)),
+                  &s.tbar[b]);
+        bulk_load(s.recb + b * TR, o.pt_rec + r0, (uint32_t)(nr * sizeof(double4)), &s.tbar[b]);
+    };
+    if (tid == 0) {
+        tissue(0);
+        if (ntile > 1) tissue(1);
     }
+    bool timeout = false;
+    for (int t = 0; t < ntile; ++t) {
+        const int b = t & 1, r0 = t * TR, nrows = min(TR, np - r0);
+        tmark(p, s, T_TILES);
+        if (!mbar_wait(&s.tbar[b], (uint32_t)((s.ctl[C_TUSE + b] + (t >> 1)) & 1))) timeout = true;
+        tmark(p, s, T_TWAIT);
+        const double *rb = s.raw + (size_t)b * TR * RS;
+        const double4 *rc = s.recb + b * TR;
+        // per-row scalars: lane k < rpw computes row warp * rpw + k
+        double dyL = 0.0, wL = 0.0, coefL = 0.0, subL = 0.0;
+        int curL = -1;
+        if (lane < rpw && warp * rpw + lane < nrows) {
+            const int rr = warp * rpw + lane;
+            const double4 rec = rc[rr];
+            double ymod = rb[rr * RS + ma];
+            if (rec.w != 0.0) {
+                curL = (int)rec.z;
+                coefL = s.ccoef[curL];
+                subL = ymod * s.crave[curL];
+                ymod = coefL * ymod;
+            }
+            dyL = rec.x - ymod;
+            wL = rec.y;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k >= rpw) break;
+            const int rr = warp * rpw + k;
+            const bool valid = rr < nrows;
+            const double dy = __shfl_sync(0xffffffffu, dyL, k);
+            const double w = __shfl_sync(0xffffffffu, wL, k);
+            const double coef = __shfl_sync(0xffffffffu, coefL, k);
+            const double sub = __shfl_sync(0xffffffffu, subL, k);
+            const int cur = __shfl_sync(0xffffffffu, curL, k);
+            const double *dav = cstat + (size_t)max(cur, 0) * CS;
+            const double *rrow = rb + rr * RS;
+            double *trow = s.T + rr * mfp, *twrow = s.TW + rr * mfp;
+            double v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = lane + 32 * u;
+                v[u] = 0.0;
+                if (valid && j < mfit) {
+                    const int col = s.fidx[j] - 1;
+                    const double raw = rrow[col];
+                    v[u] = (cur >= 0) ? coef * (raw - sub * dav[col]) : raw;
+                } else if (valid && j == mfit) {
+                    v[u] = dy;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int j = lane + 32 * u;
+                if (j < mfp) {
+                    trow[j] = v[u];
+                    twrow[j] = v[u] * w;
+                }
+            }
+        }
+        __syncthreads();
+        tmark(p, s, T_TSTAGE);
+        if (tid == 0 && t + 2 < ntile) tissue(t + 2);
+        syrk_update(s, nrows, acc);
+        __syncthreads();
+        tmark(p, s, T_TSYRK);
+    }
+    if (timeout) s.ctl[C_TIMEOUT] = 1;
+    if (tid == 0) {
+        s.ctl[C_TUSE + 0] += (ntile + 1) / 2;
+        s.ctl[C_TUSE + 1] += ntile / 2;
+    }
+    tmark(p, s, T_TILES);
 
     // convexity regularisation pseudo-points (mrqcof_curve1_last_opt, Start.cu:2539-2612)
     {
@@ -672,9 +964,7 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
                 dk[1] += (fr.w * fr.y) * y;
                 dk[2] += (fr.w * fr.z) * y;
             }
-            s.colbuf[tid] = 0.0;
         }
-        // stage: param k (1-based k+1) maps to fit slot j via fidx; non-shape columns are 0
         const double wps = conw_r * conw_r;
         for (int idx = tid; idx < kTile * mfp; idx += kThreads) {
             s.T[idx] = 0.0;
@@ -682,8 +972,7 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
         }
         __syncthreads();
         if (tid < nc) {
-            // fit slot of parameter tid+1, if fitted
-            int slot = -1;
+            int slot = -1;  // fit slot of parameter tid + 1, if fitted
             for (int j = 0; j < mfit; ++j)
                 if (s.fidx[j] == tid + 1) slot = j;
             if (slot >= 0)
@@ -693,162 +982,140 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
                 }
         }
         if (tid < 3) {
-            s.rdy[tid] = 0.0 - ym[tid];
-            s.rw[tid] = wps;
+            const double dy = 0.0 - ym[tid];
+            s.T[tid * mfp + mfit] = dy;
+            s.TW[tid * mfp + mfit] = dy * wps;
         }
         __syncthreads();
-        tile_update(s, mfit, 3, acc, beta_j, chisq);
+        syrk_update(s, 3, acc);
     }
-
-    // write alpha (lower triangle mirrored), beta, chi^2
-#pragma unroll
-    for (int i = 0; i < kBPT; ++i) {
-        if (i < acc.nb) {
-            const int j0 = 2 * acc.bj[i], k0 = 2 * acc.bk[i];
-            const int ld = s.ld;
-            const double a00 = acc.v[i][0], a01 = acc.v[i][1], a10 = acc.v[i][2], a11 = acc.v[i][3];
-            if (j0 == k0) {
-                dst[j0 * ld + j0] = a00;
-                if (j0 + 1 < mfit) {
-                    dst[(j0 + 1) * ld + j0] = a10;
-                    dst[j0 * ld + j0 + 1] = a10;
-                    dst[(j0 + 1) * ld + j0 + 1] = a11;
-                }
-            } else {
-                dst[j0 * ld + k0] = a00;
-                dst[k0 * ld + j0] = a00;
-                if (k0 + 1 < mfit) {
-                    dst[j0 * ld + k0 + 1] = a01;
-                    dst[(k0 + 1) * ld + j0] = a01;
-                }
-                if (j0 + 1 < mfit) {
-                    dst[(j0 + 1) * ld + k0] = a10;
-                    dst[k0 * ld + j0 + 1] = a10;
-                    if (k0 + 1 < mfit) {
-                        dst[(j0 + 1) * ld + k0 + 1] = a11;
-                        dst[(k0 + 1) * ld + j0 + 1] = a11;
-                    }
-                }
-            }
-        }
-    }
-    if (tid < mfit) dvec[tid] = beta_j;
-    if (tid == 0) s.scal[S_TRIAL] = chisq;
-    __syncthreads();
+    syrk_store(s, mfit, acc, dst, dvec, rows + scratch_gpart(o.n_points, RS, o.n_curves, ma));
+    tmark(p, s, T_PSEUDO);
+    if (p.phase_cycles && tid == 0) atomicAdd(&p.phase_cycles[T_NPHASE], 1ull);
     return s.scal[S_TRIAL];
 }
 
 // ---------------------------------------------------------------- LM step
 
 // Full-pivot Gauss-Jordan on covar (n x n, stride ld) and b = da
-// (mrqmin_1_end_opt, Start.cu:2880-3006).  Pivot: last maximum |a| in
-// row-major order over unpivoted rows and columns.  Returns the error code.
+// (mrqmin_1_end_opt, Start.cu:2880-3006).  The pivot is the maximum |a| over
+// unpivoted rows and columns; among equal values the last one in row-major
+// order wins, as in the serial scan: all threads search (64 row slots x 4
+// column phases) and reduce on (|a|, j*n + k), which selects exactly that
+// element.  The inverse is not needed, so already-pivoted columns are left
+// stale.  Returns the reference's error code: 0, 1 (pivot bookkeeping) or 2
+// (zero pivot).  All threads must call it.
 static __device__ int gauss_jordan(const Sh &s, int n)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ld = s.ld;
+    const int rsub = tid >> 2, csub = tid & 3;
     double *A = s.covar, *b = s.da;
-    if (tid < n) s.ipiv[tid] = 0;
+    int *ipiv = s.ipiv;
+    if (tid < n) ipiv[tid] = 0;
     if (tid == 0) s.ctl[C_ERR] = 0;
     __syncthreads();
+    int err = 0;
     for (int i = 0; i < n; ++i) {
-        // pivot search: thread j scans row j
         double big = -1.0;
-        int jr = 0, kc = 0;
-        if (tid < n && s.ipiv[tid] != 1) {
-            const double *row = A + tid * ld;
-            for (int k = 0; k < n; ++k) {
-                const int ik = s.ipiv[k];
+        int key = 0;
+        bool bad = false;
+        for (int j = rsub; j < n; j += kThreads / 4) {
+            if (ipiv[j] == 1) continue;
+            const double *row = A + j * ld;
+            for (int k = csub; k < n; k += 4) {
+                const int ik = ipiv[k];
                 if (ik == 0) {
                     const double t = fabs(row[k]);
                     if (t >= big) {
                         big = t;
-                        jr = tid;
-                        kc = k;
+                        key = j * n + k;
                     }
                 } else if (ik > 1) {
-                    s.ctl[C_ERR] = 1;
+                    bad = true;
                 }
             }
         }
-        // CTA argmax on (big, row); ties go to the larger row
+        if (bad) s.ctl[C_ERR] = 1;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
-            const double ob = __shfl_down_sync(0xffffffffu, big, off);
-            const int oj = __shfl_down_sync(0xffffffffu, jr, off);
-            const int ok = __shfl_down_sync(0xffffffffu, kc, off);
-            if (ob > big || (ob == big && oj > jr)) {
+            const double ob = __shfl_xor_sync(0xffffffffu, big, off);
+            const int ok = __shfl_xor_sync(0xffffffffu, key, off);
+            if (ob > big || (ob == big && ok > key)) {
                 big = ob;
-                jr = oj;
-                kc = ok;
+                key = ok;
             }
         }
         if (lane == 0) {
             s.red[warp * 4 + 0] = big;
-            s.red[warp * 4 + 1] = (double)jr;
-            s.red[warp * 4 + 2] = (double)kc;
+            s.red[warp * 4 + 1] = (double)key;
         }
         __syncthreads();
-        if (s.ctl[C_ERR]) break;
-        if (tid == 0) {
-            double bb = s.red[0];
-            int bjr = (int)s.red[1], bkc = (int)s.red[2];
-            for (int w = 1; w < kWarps; ++w) {
-                const double ob = s.red[w * 4];
-                const int oj = (int)s.red[w * 4 + 1];
-                if (ob > bb || (ob == bb && oj > bjr)) {
-                    bb = ob;
-                    bjr = oj;
-                    bkc = (int)s.red[w * 4 + 2];
-                }
-            }
-            if (bb < 0.0) {  // nothing but NaN left: same fallback as the serial scan
-                bjr = 0;
-                bkc = 0;
-            }
-            s.ipiv[bkc] += 1;
-            s.ctl[C_IROW] = bjr;
-            s.ctl[C_ICOL] = bkc;
+        if (s.ctl[C_ERR]) {
+            err = 1;
+            break;
         }
+        double bb = s.red[0];
+        int bkey = (int)s.red[1];
+        for (int w = 1; w < kWarps; ++w) {
+            const double ob = s.red[w * 4];
+            const int ok = (int)s.red[w * 4 + 1];
+            if (ob > bb || (ob == bb && ok > bkey)) {
+                bb = ob;
+                bkey = ok;
+            }
+        }
+        if (bb < 0.0) bkey = 0;  // nothing but NaN left: the serial scan's (0, 0)
+        const int irow = bkey / n, icol = bkey - irow * n;
+        const double piv = A[irow * ld + icol];
+        double row_r = 0.0, row_c = 0.0, colv = 0.0;
+        if (tid < n) {
+            row_r = A[irow * ld + tid];
+            row_c = A[icol * ld + tid];
+            colv = (tid == irow) ? A[icol * ld + icol] : A[tid * ld + icol];
+        }
+        const double b_r = b[irow], b_c = b[icol];
         __syncthreads();
-        const int irow = s.ctl[C_IROW], icol = s.ctl[C_ICOL];
-        if (irow != icol) {
-            for (int l = tid; l < n; l += kThreads) {
-                const double t = A[irow * ld + l];
-                A[irow * ld + l] = A[icol * ld + l];
-                A[icol * ld + l] = t;
+        if (piv == 0.0) {
+            err = 2;
+            // the reference swaps the rows before it meets the zero pivot
+            if (tid < n) {
+                A[irow * ld + tid] = row_c;
+                A[icol * ld + tid] = row_r;
             }
             if (tid == 0) {
-                const double t = b[irow];
-                b[irow] = b[icol];
-                b[icol] = t;
+                b[irow] = b_c;
+                b[icol] = b_r;
             }
-        }
-        __syncthreads();
-        const double piv = A[icol * ld + icol];
-        if (piv == 0.0) {
-            if (tid == 0) s.ctl[C_ERR] = 2;
             __syncthreads();
             break;
         }
         const double pivinv = 1.0 / piv;
-        __syncthreads();
-        for (int l = tid; l < n; l += kThreads) A[icol * ld + l] = (l == icol) ? pivinv : A[icol * ld + l] * pivinv;
-        if (tid == 0) b[icol] *= pivinv;
-        for (int ll = tid; ll < n; ll += kThreads) s.colbuf[ll] = A[ll * ld + icol];
+        if (tid < n) {
+            A[irow * ld + tid] = row_c;
+            A[icol * ld + tid] = (tid == icol) ? pivinv : row_r * pivinv;
+            s.colbuf[tid] = colv;
+        }
+        if (tid == 0) {
+            ipiv[icol] += 1;
+            b[irow] = b_c;
+            b[icol] = b_r * pivinv;
+        }
         __syncthreads();
         // eliminate: only unpivoted columns feed later pivots and b
-        for (int idx = tid; idx < n * n; idx += kThreads) {
-            const int ll = idx / n, l = idx - ll * n;
-            if (ll == icol || s.ipiv[l] != 0) continue;
-            A[ll * ld + l] -= A[icol * ld + l] * s.colbuf[ll];
+        const double *prow = A + icol * ld;
+        for (int ll = rsub; ll < n; ll += kThreads / 4) {
+            if (ll == icol) continue;
+            const double cb = s.colbuf[ll];
+            double *row = A + ll * ld;
+            for (int l = csub; l < n; l += 4)
+                if (ipiv[l] == 0) row[l] -= prow[l] * cb;
         }
-        for (int ll = tid; ll < n; ll += kThreads)
-            if (ll != icol) b[ll] -= b[icol] * s.colbuf[ll];
+        const double bi = b[icol];
+        if (tid < n && tid != icol) b[tid] -= bi * s.colbuf[tid];
         __syncthreads();
     }
-    __syncthreads();
-    return s.ctl[C_ERR];
+    return err;
 }
 
 // ---------------------------------------------------------------- kernel
@@ -860,20 +1127,27 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Sh s;
-    carve_bytes(o.n_fac, o.mfit, o.ncp, &s, smem_raw);
+    carve_bytes(o.n_fac, o.mfit, o.ncp, o.n_curves, o.row_stride, o.tile_rows, o.cstat_smem, &s, smem_raw);
     const int tid = threadIdx.x;
     const int nc = o.n_coef, ma = o.ma, mfit = o.mfit, ld = s.ld;
     double *rows = scratch + (size_t)blockIdx.x * scratch_per_cta;
     double *cstat = rows + (size_t)o.n_points * o.row_stride;
-    int *perm = reinterpret_cast<int *>(cstat + (size_t)o.n_curves * (ma + 3));  // [2][n_points]
+    int *perm = reinterpret_cast<int *>(rows + scratch_perm(o.n_points, o.row_stride, o.n_curves, ma));
 
     for (int f = tid; f < o.n_fac; f += kThreads) s.F[f] = ldg4(&o.facet[f]);
     if (tid < mfit) s.fidx[tid] = __ldg(&o.fidx[tid]);
     if (tid == 0) {
-        mbar_init(&s.mbar[0], 1);
-        mbar_init(&s.mbar[1], 1);
-        s.ctl[C_YUSE0] = 0;
-        s.ctl[C_YUSE1] = 0;
+        for (int b = 0; b < kStages; ++b) {
+            mbar_init(&s.mbar[b], 1);
+            s.ctl[C_YUSE + b] = 0;
+            s.ctl[C_REL + b] = 0;
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&s.tbar[b], 2);  // two copies (rows + records) per fill
+            s.ctl[C_TUSE + b] = 0;
+        }
+        for (int q = 0; q < T_NPHASE; ++q) s.tclk[q] = 0;
+        s.tclk[T_NPHASE] = clock64();
         s.ctl[C_TIMEOUT] = 0;
     }
     __syncthreads();
@@ -952,7 +1226,9 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
             }
             if (tid < mfit) s.da[tid] = s.beta[tid];
             __syncthreads();
+            tmark(p, s, T_REST);
             const int err = gauss_jordan(s, mfit);
+            tmark(p, s, T_SOLVE);
             if (err == 0 || err == 2) {
                 if (tid < mfit) s.atry[s.fidx[tid]] = s.a[s.fidx[tid]] + s.da[tid];
                 if (err == 2 && tid == 0) s.ctl[C_STATUS] |= kStatusSingular;
@@ -1027,6 +1303,13 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
             r.status = s.ctl[C_STATUS] | (s.ctl[C_TIMEOUT] ? kStatusTimeout : 0);
             out[item] = r;
             if (r.status) atomicOr(status, r.status);
+            if (p.phase_cycles) {
+                tmark(p, s, T_REST);
+                for (int q = 0; q < T_NPHASE; ++q) {
+                    atomicAdd(&p.phase_cycles[q], (unsigned long long)s.tclk[q]);
+                    s.tclk[q] = 0;
+                }
+            }
         }
         __syncthreads();
         if (s.ctl[C_TIMEOUT]) break;  // a bulk copy never completed: stop taking items
@@ -1034,8 +1317,8 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
     // after a timeout, give any copy still in flight a bounded chance to land
     // before the CTA's shared memory is released
     if (tid == 0 && s.ctl[C_TIMEOUT]) {
-        mbar_wait(&s.mbar[0], (uint32_t)(s.ctl[C_YUSE0] & 1));
-        mbar_wait(&s.mbar[1], (uint32_t)(s.ctl[C_YUSE1] & 1));
+        for (int b = 0; b < kStages; ++b) mbar_wait(&s.mbar[b], (uint32_t)(s.ctl[C_YUSE + b] & 1));
+        for (int b = 0; b < 2; ++b) mbar_wait(&s.tbar[b], (uint32_t)(s.ctl[C_TUSE + b] & 1));
     }
 }
 

@@ -63,6 +63,7 @@ _SIGS = {
     "ps_gpu_eval": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     "ps_gpu_status": (C.c_int, [C.c_void_p, _ip]),
     "ps_gpu_set_quirks": (C.c_int, [C.c_void_p, C.c_int32]),
+    "ps_gpu_phase_clocks": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
     "ps_gpu_stream": (C.c_void_p, [C.c_void_p]),
     "ps_gpu_occupancy": (C.c_int, [C.c_void_p, _ip, _ip]),
     "ps_setup_shape": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
@@ -246,6 +247,17 @@ class Engine:
         f = np.zeros(1, dtype=np.int32)
         _check(lib().ps_gpu_status(self.h, _p(f, C.c_int32)))
         return int(f[0])
+
+    PHASES = ("curv", "sort", "sweep", "curve_stats", "jtwj_other", "pseudo", "solve", "rest", "tile_wait",
+              "tile_stage", "tile_syrk")
+
+    def phase_clocks(self, enable=True):
+        """Cycles per phase since the last call (dict), then restarts counting."""
+        out = np.zeros(12, dtype=np.int64)
+        _check(lib().ps_gpu_phase_clocks(self.h, 1 if enable else 0, out.ctypes.data_as(C.POINTER(C.c_int64))))
+        d = dict(zip(self.PHASES, out[:11].tolist()))
+        d["evals"] = int(out[11])
+        return d
 
     def occupancy(self):
         a = np.zeros(1, dtype=np.int32)
