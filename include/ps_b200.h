@@ -177,6 +177,9 @@ int32_t ps_n_coef(int32_t l_max, int32_t m_max);
 /* FP64 FMA throughput of the device in TFLOP/s (the compute roofline of the
    fit kernel; no reference counterpart). */
 ps_status ps_measure_fp64_peak(int32_t device, double *tflops);
+/* Test hook: r[i] = the fit kernel's branch-free reciprocal of d[i], on the
+   current device (no reference counterpart). */
+ps_status ps_probe_reciprocal(int32_t n, const double *d, double *r);
 
 const char *ps_last_error(void);
 const char *ps_version(void);

@@ -21,6 +21,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "devmath.cuh"
 #include "engine.h"
 
 namespace psb {
@@ -533,41 +534,48 @@ __device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows, c
                 const double *yb = s.ybuf + (size_t)b * fc * NCP;
 #pragma unroll 1
                 for (int k0 = 0; k0 < nfc; k0 += 4) {
-                    double wk[4];
-                    bool any4 = false;
+                    // four facets per step: visibility first, one vote, then four
+                    // independent branch-free chains the scheduler can interleave
+                    double4 fr[4];
+                    double mu[4], mu0[4];
+                    bool vis[4];
+                    bool v4 = false;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        wk[q] = 0.0;
-                        if (k0 + q < nfc) {
-                            const double4 fr = s.F[f0 + k0 + q];
-                            const double mu = ex * fr.x + ey * fr.y + ez * fr.z;
-                            const double mu0 = sx * fr.x + sy * fr.y + sz * fr.z;
-                            const bool vis = act && (mu > kTiny) && (mu0 > kTiny);
-                            if (__any_sync(0xffffffffu, vis)) {
-                                // lanes that do not see the facet run the same arithmetic on
-                                // finite stand-ins and contribute exact zeros
-                                const double ar = vis ? fr.w : 0.0;
-                                const double r = __drcp_rn(vis ? mu + mu0 : 1.0);
-                                const double sv = mu * mu0 * (cl + cls * r);
-                                const double q0 = mu0 * r, q1 = mu * r;
-                                const double dsmu = cls * (q0 * q0) + cl * mu0;
-                                const double dsmu0 = cls * (q1 * q1) + cl * mu;
-                                const double amm = ar * mu * mu0;
-                                const double w = ar * sv;
-                                const double gg = ar * dsmu;
-                                const double g0 = ar * dsmu0;
-                                br += w;
-                                u0 = fma(gg, fr.x, u0);
-                                u1 = fma(gg, fr.y, u1);
-                                u2 = fma(gg, fr.z, u2);
-                                w0 = fma(g0, fr.x, w0);
-                                w1 = fma(g0, fr.y, w1);
-                                w2 = fma(g0, fr.z, w2);
-                                t4 += amm;
-                                t5 += amm * r;
-                                wk[q] = w;
-                                any4 = true;
-                            }
+                        const bool inside = k0 + q < nfc;
+                        fr[q] = s.F[f0 + (inside ? k0 + q : 0)];
+                        mu[q] = ex * fr[q].x + ey * fr[q].y + ez * fr[q].z;
+                        mu0[q] = sx * fr[q].x + sy * fr[q].y + sz * fr[q].z;
+                        vis[q] = act && inside && (mu[q] > kTiny) && (mu0[q] > kTiny);
+                        v4 = v4 || vis[q];
+                    }
+                    const bool any4 = __any_sync(0xffffffffu, v4);
+                    double wk[4] = {0.0, 0.0, 0.0, 0.0};
+                    if (any4) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            // lanes that do not see the facet run the same arithmetic on
+                            // finite stand-ins and contribute exact zeros
+                            const double ar = vis[q] ? fr[q].w : 0.0;
+                            const double r = rcp_nr(vis[q] ? mu[q] + mu0[q] : 1.0);
+                            const double sv = mu[q] * mu0[q] * (cl + cls * r);
+                            const double q0 = mu0[q] * r, q1 = mu[q] * r;
+                            const double dsmu = cls * (q0 * q0) + cl * mu0[q];
+                            const double dsmu0 = cls * (q1 * q1) + cl * mu[q];
+                            const double amm = ar * mu[q] * mu0[q];
+                            const double w = ar * sv;
+                            const double gg = ar * dsmu;
+                            const double g0 = ar * dsmu0;
+                            br += w;
+                            u0 = fma(gg, fr[q].x, u0);
+                            u1 = fma(gg, fr[q].y, u1);
+                            u2 = fma(gg, fr[q].z, u2);
+                            w0 = fma(g0, fr[q].x, w0);
+                            w1 = fma(g0, fr[q].y, w1);
+                            w2 = fma(g0, fr[q].z, w2);
+                            t4 += amm;
+                            t5 += amm * r;
+                            wk[q] = w;
                         }
                     }
                     if (any4) {  // warp-uniform

@@ -3,6 +3,7 @@
 // keep the FP64 pipe busy; returns achieved TFLOP/s (2 FLOP per FMA).
 #include <cuda_runtime.h>
 
+#include "devmath.cuh"
 #include "ps_b200.h"
 #include "util.h"
 
@@ -27,7 +28,30 @@ __global__ void __launch_bounds__(256) fma_probe(double *out, double x)
     if (t == 12345.678) out[blockIdx.x] = t;  // never true; keeps the work live
 }
 
+__global__ void rcp_probe(const double *d, double *r, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = psb::rcp_nr(d[i]);
+}
+
 }  // namespace
+
+extern "C" ps_status ps_probe_reciprocal(int32_t n, const double *d, double *r)
+{
+    if (n <= 0 || !d || !r) return psb_fail(PS_ERR_ARG, "ps_probe_reciprocal: bad arguments");
+    double *dd = nullptr;
+    cudaError_t e = cudaMalloc(&dd, sizeof(double) * 2 * (size_t)n);
+    if (e != cudaSuccess) return psb_fail_cuda(e, "cudaMalloc");
+    e = cudaMemcpy(dd, d, sizeof(double) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        rcp_probe<<<(n + 255) / 256, 256>>>(dd, dd + n, n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(r, dd + n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaFree(dd);
+    if (e != cudaSuccess) return psb_fail_cuda(e, "ps_probe_reciprocal");
+    return PS_OK;
+}
 
 extern "C" ps_status ps_measure_fp64_peak(int32_t device, double *tflops)
 {

@@ -70,6 +70,7 @@ _SIGS = {
                                  _dp, _dp, _dp, _dp]),
     "ps_n_coef": (C.c_int32, [C.c_int32, C.c_int32]),
     "ps_measure_fp64_peak": (C.c_int, [C.c_int32, _dp]),
+    "ps_probe_reciprocal": (C.c_int, [C.c_int32, _dp, _dp]),
     "ps_last_error": (C.c_char_p, []),
     "ps_version": (C.c_char_p, []),
 }
@@ -125,6 +126,13 @@ def measure_fp64_peak(device=0):
     t = np.zeros(1)
     _check(lib().ps_measure_fp64_peak(device, _p(t)))
     return float(t[0])
+
+
+def probe_reciprocal(d):
+    d = np.ascontiguousarray(d, dtype=np.float64)
+    r = np.zeros_like(d)
+    _check(lib().ps_probe_reciprocal(len(d), _p(d), _p(r)))
+    return r
 
 
 class Engine:

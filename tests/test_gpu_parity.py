@@ -156,3 +156,16 @@ def test_status_and_argument_errors():
         g, _, st = eng.fit_items(np.array([1, 2]), np.array([0, 1]))
         assert np.all(np.isfinite(g[:, 0]))
         assert eng.status() & native.DEVSTAT_NAN_CHISQ == 0
+
+
+def test_branch_free_reciprocal_within_one_ulp():
+    """The facet sweep's reciprocal (rcp.approx seed + two Newton steps) vs the
+    correctly rounded 1/d over the argument range it sees, (2e-8, 2]."""
+    from ps_claude_opt_b200 import native
+
+    rng = np.random.default_rng(5)
+    d = np.concatenate([np.exp(rng.uniform(np.log(2e-8), np.log(2.0), 200000)), [2e-8, 1.0, 2.0, 0.5, 1e-3]])
+    r = native.probe_reciprocal(d)
+    exact = 1.0 / d
+    ulp = np.spacing(exact)
+    assert np.all(np.abs(r - exact) <= ulp)
