@@ -41,7 +41,8 @@ enum { C_ITEM, C_NITER, C_STATUS, C_ERR, C_IROW, C_ICOL, C_GO, C_ACCEPT, C_TIMEO
        C_YUSE,                       // [kStages] completed uses of each chunk buffer
        C_REL = C_YUSE + kStages,     // [kStages] warps done with the chunk in each buffer
        C_TUSE = C_REL + kStages,     // [2] completed uses of each J^T W J tile buffer
-       C_NCTL = C_TUSE + 2 };
+       C_TREL = C_TUSE + 2,          // [2] warps done with each tile buffer (k-slice mode)
+       C_NCTL = C_TREL + 2 };
 // per-CTA phase clocks (optional instrumentation)
 enum { T_CURV, T_SORT, T_SWEEP, T_CSTAT, T_TILES, T_PSEUDO, T_SOLVE, T_REST, T_TWAIT, T_TSTAGE, T_TSYRK,
        T_NPHASE };
@@ -879,6 +880,75 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
         if (ntile > 1) tissue(1);
     }
     bool timeout = false;
+    if (acc.slice) {
+        // k-slice mode: warp w owns rows 4w..4w+3 of every tile and builds its
+        // MMA fragments straight from the raw rows in shared memory (lane row
+        // 4w + lane%4, fit column 8q + lane/4), so the tile loop needs no CTA
+        // barrier; the last warp done with a buffer refills it
+        const int rr = 4 * warp + (lane & 3);
+        const int jl = lane >> 2;
+        for (int t = 0; t < ntile; ++t) {
+            const int b = t & 1, r0 = t * TR, nrows = min(TR, np - r0);
+            tmark(p, s, T_TILES);
+            if (!mbar_wait(&s.tbar[b], (uint32_t)((s.ctl[C_TUSE + b] + (t >> 1)) & 1))) timeout = true;
+            tmark(p, s, T_TWAIT);
+            if (4 * warp < nrows) {
+                const double *rb = s.raw + (size_t)b * TR * RS;
+                const bool valid = rr < nrows;
+                double dy = 0.0, w = 0.0, coef = 0.0, sub = 0.0;
+                int cur = -1;
+                if (valid) {
+                    const double4 rec = s.recb[b * TR + rr];
+                    double ymod = rb[rr * RS + ma];
+                    if (rec.w != 0.0) {
+                        cur = (int)rec.z;
+                        coef = s.ccoef[cur];
+                        sub = ymod * s.crave[cur];
+                        ymod = coef * ymod;
+                    }
+                    dy = rec.x - ymod;
+                    w = rec.y;
+                }
+                const double *dav = cstat + (size_t)max(cur, 0) * CS;
+                const double *rrow = rb + rr * RS;
+                double fa[8], fb[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int j = 8 * q + jl;
+                    double v = 0.0;
+                    if (valid && q < acc.nb) {
+                        if (j < mfit) {
+                            const int col = s.fidx[j] - 1;
+                            const double raw = rrow[col];
+                            v = (cur >= 0) ? coef * (raw - sub * dav[col]) : raw;
+                        } else if (j == mfit) {
+                            v = dy;
+                        }
+                    }
+                    fb[q] = v;
+                    fa[q] = v * w;
+                }
+#pragma unroll
+                for (int bj = 0; bj < 8; ++bj)
+#pragma unroll
+                    for (int bk = 0; bk <= bj; ++bk)
+                        if (bj < acc.nb) {
+                            const int i = bj * (bj + 1) / 2 + bk;
+                            dmma_8x8x4(acc.c[i][0], acc.c[i][1], fa[bj], fb[bk]);
+                        }
+            }
+            tmark(p, s, T_TSYRK);
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                if (atomicAdd(&s.ctl[C_TREL + b], 1) == kWarps - 1) {
+                    s.ctl[C_TREL + b] = 0;
+                    if (t + 2 < ntile) tissue(t + 2);
+                }
+            }
+        }
+        __syncthreads();
+    } else {
     for (int t = 0; t < ntile; ++t) {
         const int b = t & 1, r0 = t * TR, nrows = min(TR, np - r0);
         tmark(p, s, T_TILES);
@@ -944,6 +1014,7 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
         __syncthreads();
         tmark(p, s, T_TSYRK);
     }
+    }
     if (timeout) s.ctl[C_TIMEOUT] = 1;
     if (tid == 0) {
         s.ctl[C_TUSE + 0] += (ntile + 1) / 2;
@@ -1008,11 +1079,13 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
 // Full-pivot Gauss-Jordan on covar (n x n, stride ld) and b = da
 // (mrqmin_1_end_opt, Start.cu:2880-3006).  The pivot is the maximum |a| over
 // unpivoted rows and columns; among equal values the last one in row-major
-// order wins, as in the serial scan: all threads search (64 row slots x 4
-// column phases) and reduce on (|a|, j*n + k), which selects exactly that
-// element.  The inverse is not needed, so already-pivoted columns are left
-// stale.  Returns the reference's error code: 0, 1 (pivot bookkeeping) or 2
-// (zero pivot).  All threads must call it.
+// order wins, as in the serial scan: threads (64 row slots x 4 column phases)
+// keep a local candidate (|a|, j*n + k) and the CTA reduces on it, which
+// selects exactly that element.  The candidate search for pivot i+1 runs
+// inside the elimination of pivot i, on the values just written.  The inverse
+// is not needed, so already-pivoted columns are left stale.  Returns the
+// reference's error code: 0, 1 (pivot bookkeeping) or 2 (zero pivot).  All
+// threads must call it.
 static __device__ int gauss_jordan(const Sh &s, int n)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1021,30 +1094,22 @@ static __device__ int gauss_jordan(const Sh &s, int n)
     double *A = s.covar, *b = s.da;
     int *ipiv = s.ipiv;
     if (tid < n) ipiv[tid] = 0;
-    if (tid == 0) s.ctl[C_ERR] = 0;
     __syncthreads();
-    int err = 0;
-    for (int i = 0; i < n; ++i) {
-        double big = -1.0;
-        int key = 0;
-        bool bad = false;
-        for (int j = rsub; j < n; j += kThreads / 4) {
-            if (ipiv[j] == 1) continue;
-            const double *row = A + j * ld;
-            for (int k = csub; k < n; k += 4) {
-                const int ik = ipiv[k];
-                if (ik == 0) {
-                    const double t = fabs(row[k]);
-                    if (t >= big) {
-                        big = t;
-                        key = j * n + k;
-                    }
-                } else if (ik > 1) {
-                    bad = true;
-                }
+    double big = -1.0;
+    int key = 0;
+    for (int j = rsub; j < n; j += kThreads / 4) {
+        const double *row = A + j * ld;
+        for (int k = csub; k < n; k += 4) {
+            const double t = fabs(row[k]);
+            if (t >= big) {
+                big = t;
+                key = j * n + k;
             }
         }
-        if (bad) s.ctl[C_ERR] = 1;
+    }
+    bool bad = false;
+    int err = 0;
+    for (int i = 0; i < n; ++i) {
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             const double ob = __shfl_xor_sync(0xffffffffu, big, off);
@@ -1054,24 +1119,28 @@ static __device__ int gauss_jordan(const Sh &s, int n)
                 key = ok;
             }
         }
+        const bool wbad = __any_sync(0xffffffffu, bad);
         if (lane == 0) {
             s.red[warp * 4 + 0] = big;
             s.red[warp * 4 + 1] = (double)key;
+            s.red[warp * 4 + 2] = wbad ? 1.0 : 0.0;
         }
         __syncthreads();
-        if (s.ctl[C_ERR]) {
-            err = 1;
-            break;
-        }
         double bb = s.red[0];
         int bkey = (int)s.red[1];
+        bool anybad = s.red[2] != 0.0;
         for (int w = 1; w < kWarps; ++w) {
             const double ob = s.red[w * 4];
             const int ok = (int)s.red[w * 4 + 1];
+            anybad = anybad || s.red[w * 4 + 2] != 0.0;
             if (ob > bb || (ob == bb && ok > bkey)) {
                 bb = ob;
                 bkey = ok;
             }
+        }
+        if (anybad) {
+            err = 1;
+            break;
         }
         if (bb < 0.0) bkey = 0;  // nothing but NaN left: the serial scan's (0, 0)
         const int irow = bkey / n, icol = bkey - irow * n;
@@ -1110,19 +1179,50 @@ static __device__ int gauss_jordan(const Sh &s, int n)
             b[icol] = b_r * pivinv;
         }
         __syncthreads();
-        // eliminate: only unpivoted columns feed later pivots and b
+        // eliminate (only unpivoted columns feed later pivots and b) and look
+        // for the next pivot among unpivoted rows and columns
+        big = -1.0;
+        key = 0;
+        bad = false;
         const double *prow = A + icol * ld;
         for (int ll = rsub; ll < n; ll += kThreads / 4) {
-            if (ll == icol) continue;
-            const double cb = s.colbuf[ll];
+            const bool open_row = ipiv[ll] != 1;
             double *row = A + ll * ld;
-            for (int l = csub; l < n; l += 4)
-                if (ipiv[l] == 0) row[l] -= prow[l] * cb;
+            if (ll == icol) {
+                if (open_row)  // only after a bookkeeping fault: keep the serial checks
+                    for (int l = csub; l < n; l += 4) {
+                        const int il = ipiv[l];
+                        if (il == 0) {
+                            const double t = fabs(row[l]);
+                            if (t >= big) { big = t; key = ll * n + l; }
+                        } else if (il > 1) {
+                            bad = true;
+                        }
+                    }
+                continue;
+            }
+            const double cb = s.colbuf[ll];
+            for (int l = csub; l < n; l += 4) {
+                const int il = ipiv[l];
+                if (il == 0) {
+                    const double v = row[l] - prow[l] * cb;
+                    row[l] = v;
+                    if (open_row) {
+                        const double t = fabs(v);
+                        if (t >= big) {
+                            big = t;
+                            key = ll * n + l;
+                        }
+                    }
+                } else if (il > 1 && open_row) {
+                    bad = true;
+                }
+            }
         }
         const double bi = b[icol];
         if (tid < n && tid != icol) b[tid] -= bi * s.colbuf[tid];
-        __syncthreads();
     }
+    __syncthreads();
     return err;
 }
 
@@ -1153,6 +1253,7 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
         for (int b = 0; b < 2; ++b) {
             mbar_init(&s.tbar[b], 2);  // two copies (rows + records) per fill
             s.ctl[C_TUSE + b] = 0;
+            s.ctl[C_TREL + b] = 0;
         }
         for (int q = 0; q < T_NPHASE; ++q) s.tclk[q] = 0;
         s.tclk[T_NPHASE] = clock64();
