@@ -168,6 +168,36 @@ void *ps_gpu_stream(ps_gpu *h);
 /* Fit CTAs resident per SM and SM count for the configured object. */
 ps_status ps_gpu_occupancy(ps_gpu *h, int32_t *ctas_per_sm, int32_t *n_sm);
 
+/* Allocation-free variant of ps_gpu_fit_items (no counterpart in the
+   reference).  For callers that cannot call cudaMalloc: a framework whose
+   own caching allocator owns the device memory (an allocation behind its back
+   can fail on a full pool or fragment it), or a pipeline that forbids
+   allocation once running (cudaMalloc can synchronise the device and stall
+   the other streams).  Takes the
+   arguments of ps_gpu_prepare + ps_gpu_configure + ps_gpu_fit_items as host
+   arrays and writes host results; allocates nothing, on the device or the
+   host heap.  All device data live in one file-scope 64 MiB __device__
+   array, present on every GPU that loads the library until the process
+   exits.  The first call on a device looks up that array's address with the
+   device current and sets the kernel's shared-memory limit: make it before
+   any stream capture.  Calls share the array and leave their data in it;
+   calls that overlap on the GPU race -- serialise them.  Objects whose tables
+   plus one CTA's scratch exceed 64 MiB, or with more than 200 lightcurves,
+   are rejected with PS_ERR_ARG; smaller ones run on as many CTAs as the
+   remaining scratch holds.  stream may be NULL (the legacy default stream);
+   the call returns after the results are in out. */
+ps_status ps_fit_items_noalloc(int32_t device, void *stream, const double *beta_pole,
+                               const double *lambda_pole, const double *par, double cl,
+                               double alamda_start, double alamda_incr, double alamda_incrr,
+                               const double *ee, const double *ee0, const double *tim, double phi0,
+                               const double *weight, double freq_start, double freq_step,
+                               double stop_condition, int32_t n_iter_min, double conw_r,
+                               double conw_r_rms, int32_t ndata, const int32_t *ia,
+                               const int32_t *ia_par, const double *cg_first, const double *sig,
+                               const double *sigr2, int32_t numfac, const double *brightness,
+                               const ps_curves *curves, const ps_shape *shape, int32_t n,
+                               const int32_t *n_freq, const int32_t *pole, ps_fit_result *out);
+
 /* Host shape setup (trifac.c, areanorm.c, sphfunc.c, ellfit.c of the
    reference): facet normals, areas, Laplace basis and the ellipsoid fit. */
 ps_status ps_setup_shape(int32_t l_max, int32_t m_max, int32_t nrows, double a, double b, double c,

@@ -68,6 +68,11 @@ _SIGS = {
     "ps_gpu_occupancy": (C.c_int, [C.c_void_p, _ip, _ip]),
     "ps_setup_shape": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                  _dp, _dp, _dp, _dp]),
+    "ps_fit_items_noalloc": (C.c_int, [C.c_int32, C.c_void_p, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, _dp, _dp, _dp, C.c_double, _dp, C.c_double, C.c_double,
+                                       C.c_double, C.c_int32, C.c_double, C.c_double, C.c_int32, _ip, _ip, _dp,
+                                       _dp, _dp, C.c_int32, _dp, C.POINTER(Curves), C.POINTER(Shape), C.c_int32,
+                                       _ip, _ip, C.POINTER(FitResult)]),
     "ps_n_coef": (C.c_int32, [C.c_int32, C.c_int32]),
     "ps_measure_fp64_peak": (C.c_int, [C.c_int32, _dp]),
     "ps_probe_reciprocal": (C.c_int, [C.c_int32, _dp, _dp]),
@@ -276,6 +281,40 @@ class Engine:
     @property
     def stream(self):
         return lib().ps_gpu_stream(self.h)
+
+
+def fit_items_noalloc(obj, n_freq, pole, device=0, conw_r=None):
+    """ps_fit_items_noalloc on a prepared object: the allocation-free variant of
+    Engine.fit_items (host inputs, host results, one static device arena)."""
+    keep = []
+
+    def arr(x, dt=np.float64):
+        a = np.ascontiguousarray(x, dtype=dt)
+        keep.append(a)
+        return a
+
+    n_freq = arr(n_freq, np.int32)
+    pole = arr(pole, np.int32)
+    n = len(n_freq)
+    res = (FitResult * max(n, 1))()
+    cw = obj.conw_r if conw_r is None else conw_r
+    curves = Curves(obj.n_curves, _p(arr(obj.curve_len, np.int32), C.c_int32),
+                    _p(arr(obj.curve_rel, np.int32), C.c_int32))
+    shape = Shape(obj.n_coef, _p(arr(obj.normal)), _p(arr(obj.d_area)), _p(arr(obj.dsph)))
+    ia = arr(obj.ia, np.int32)
+    ia_par = arr(obj.ia[obj.n_coef + 4:obj.n_coef + 7], np.int32)
+    g = obj.grid
+    _check(lib().ps_fit_items_noalloc(
+        device, None, _p(arr(obj.beta_pole)), _p(arr(obj.lambda_pole)), _p(arr(obj.par)), float(obj.cl),
+        obj.alamda_start, obj.alamda_incr, obj.alamda_incrr, _p(arr(obj.ee)), _p(arr(obj.ee0)), _p(arr(obj.tim)),
+        obj.phi0, _p(arr(obj.weight)), g.freq_start, g.freq_step, float(obj.stop_condition), obj.n_iter_min, cw, cw,
+        obj.n_points, _p(ia, C.c_int32), _p(ia_par, C.c_int32), _p(arr(obj.cg_first)), _p(arr(obj.sig)),
+        _p(arr(obj.sigr2)), obj.n_fac, _p(arr(obj.brightness)), C.byref(curves), C.byref(shape), n,
+        _p(n_freq, C.c_int32), _p(pole, C.c_int32), res))
+    out = np.array([(r.dev, r.dark, r.per, r.lambda_deg, r.beta_deg, r.chisq) for r in res[:n]])
+    niter = np.array([r.niter for r in res[:n]], dtype=np.int32)
+    status = np.array([r.status for r in res[:n]], dtype=np.int32)
+    return out.reshape(n, 6), niter, status
 
 
 def run_object(obj, device=0, quirks=0, max_freq=None, progress=None):
