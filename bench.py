@@ -34,6 +34,11 @@ sys.path.insert(0, ROOT)
 SEED = 1000003 * 2          # production config, object 0
 FITS_PER_CTA = 10           # fits per resident CTA in one step
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+# DRAM bytes per fit of the fit kernel on this workload: dram__bytes_read.sum +
+# dram__bytes_write.sum = 27.53 GB over the 148 fits of one ncu capture of
+# `bench.py --profile-case` (the derivative-row scratch round trip; it grows
+# with the number of fits, so a launch's traffic is this times its fits).
+NCU_DRAM_BYTES_PER_FIT = 27.53e9 / 148
 METRIC = "LM fits/s (FP64 full scan of the production object, 1 B200)"
 
 
@@ -313,7 +318,8 @@ def main():
                        "parallelism": "dp%d (disjoint frequency ranges per GPU)" % world},
             "s_per_object": n_obj / (value / world),
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": NCU_DRAM_BYTES_PER_FIT * n_fits,
+                         "traffic_source": "ncu capture of the profile case (148 fits), scaled by fits per launch",
                          "peak_source": "measured FP64 FMA probe (ps_measure_fp64_peak) on this GPU; "
                                         "MEASURED_PEAKS.json has no FP64 figure",
                          "flops_per_launch": fl, "mean_niter": niter},
@@ -324,10 +330,11 @@ def main():
         }
         if world == 1 and not args.no_cpu_baseline:
             cores = os.cpu_count() or 1
-            rate, cores, dt = cpu_baseline(obj, max(8, 2 * cores))
+            n_cpu = 10 * cores     # about 10 s of CPU work at ~1 fit/s per core
+            rate, cores, dt = cpu_baseline(obj, n_cpu)
             line["cpu_baseline"] = {"value": rate, "unit": "fits/s", "cores": cores, "kind": "port",
                                     "sample": "%d fits (frequencies 1.., 10 poles) of the same object, %.1f s" %
-                                              (max(8, 2 * cores), dt)}
+                                              (n_cpu, dt)}
         print(json.dumps(line), flush=True)
     eng.close()
     if dist:
