@@ -12,6 +12,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libps_b200.so")
+# the C++ host program (period_search_in -> period_search_out) built beside the library
+HOST_PROGRAM = os.path.join(HERE, "_lib", "period_search")
 
 N_POLES = 10
 QUIRK_PRECALC_CONW = 1
