@@ -125,6 +125,38 @@ ps_status ps_gpu_start(ps_gpu *h, int32_t n_start_from, double freq_start, doubl
 /* Replaces CUDAUnprepare (start_CUDA.h:16, start_CUDA.cu:368-385). */
 void ps_gpu_unprepare(ps_gpu *h);
 
+/* One object of a batch scan: the arguments that ps_gpu_prepare,
+   ps_gpu_precalc and ps_gpu_start take for it. */
+typedef struct ps_object {
+    const double *beta_pole, *lambda_pole;   /* [PS_N_POLES], degrees */
+    const double *par;                       /* [3] phase-function start values */
+    double cl, alamda_start, alamda_incr, alamda_incrr, phi0;
+    int32_t ndata;
+    const double *tim, *ee, *ee0, *weight, *brightness, *sig, *sigr2;
+    const int32_t *ia, *ia_par;
+    const double *cg_first;
+    int32_t numfac;
+    ps_curves curves;
+    ps_shape shape;
+    double freq_start, freq_end, freq_step, stop_condition;
+    int32_t n_iter_min;
+    double escl;
+    double conw_r;          /* conw / escl^2: the convexity-weight search starts here */
+    int32_t n_start_from;   /* first frequency of the scan (>= 1) */
+    int32_t max_lines;      /* lines reserved for this object in the output */
+} ps_object;
+
+/* The reference's whole flow -- convexity-weight search (CUDAPrecalc), then
+   the scan (CUDAStart) -- for n_obj objects at once (no counterpart in the
+   reference, which runs one object per process).  Each search round and the
+   scans of all objects are enqueued on a few streams, so the GPU stays full
+   while small objects' launches start and end.  Lines of object i go to
+   lines[line_offset[i] .. + n_lines[i]); the final convexity weight to
+   conw_r_out[i].  quirks: PS_QUIRK_* for every object. */
+ps_status ps_gpu_scan_batch(int32_t device, int32_t n_obj, const ps_object *objs, int32_t quirks,
+                            ps_line *lines, const int64_t *line_offset, int32_t *n_lines,
+                            double *conw_r_out);
+
 /* ---- finer-grained entry points (no reference counterpart: the reference
         keeps these steps inside CUDAStart) ---- */
 

@@ -13,36 +13,13 @@
 #include <vector>
 
 #include "engine.h"
+#include "handle.h"
 #include "ps_b200.h"
 #include "util.h"
 
 namespace {
 
 thread_local std::string g_last_error;
-
-template <typename T>
-struct DevBuf {
-    T *ptr = nullptr;
-    size_t cap = 0;
-    cudaError_t ensure(size_t n)
-    {
-        if (n <= cap && ptr) return cudaSuccess;
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        cap = 0;
-        cudaError_t e = cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(T));
-        if (e == cudaSuccess) cap = std::max<size_t>(n, 1);
-        return e;
-    }
-    void release()
-    {
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        cap = 0;
-    }
-};
-
-constexpr int kMaxIter = 60;  // constants.h:12
 
 }  // namespace
 
@@ -57,36 +34,6 @@ ps_status psb_fail_cuda(int cuda_error, const char *what)
     g_last_error = std::string(what) + ": " + cudaGetErrorString((cudaError_t)cuda_error);
     return PS_ERR_CUDA;
 }
-
-#define PSB_CUDA(call)                                         \
-    do {                                                       \
-        cudaError_t e_ = (call);                               \
-        if (e_ != cudaSuccess) return psb_fail_cuda(e_, #call); \
-    } while (0)
-
-struct ps_gpu {
-    int device = 0;
-    int n_sm = 0;
-    cudaStream_t stream = nullptr;
-    int quirks = 0;
-    // prepare-time inputs
-    int ndata = 0;
-    std::vector<double> tim, ee, ee0, weight;
-    double beta_pole[PS_N_POLES], lambda_pole[PS_N_POLES], par[3];
-    double lcl = 0, alamda_start = 0, alamda_incr = 0, alamda_incrr = 0, phi0 = 0;
-    // configured object
-    bool configured = false;
-    psb::DevObject obj{};
-    psb::DevParams prm{};
-    int ctas_per_sm = 0;
-    DevBuf<double4> facet, pt_a, pt_b, pt_rec;
-    DevBuf<double> ysh, pt_w, curve_sig, cg_first, scratch, eval_buf;
-    DevBuf<int> pt_curve, curve_start, curve_rel, fidx, queue, status;
-    DevBuf<psb::FitItem> items;
-    DevBuf<unsigned long long> phase;
-    DevBuf<psb::FitOut> out;
-    size_t scratch_per_cta = 0;
-};
 
 extern "C" const char *ps_last_error(void) { return g_last_error.c_str(); }
 extern "C" const char *ps_version(void) { return "ps-b200 0.1 (sm_100a FP64 persistent LM)"; }
@@ -156,13 +103,6 @@ extern "C" ps_status ps_gpu_set_quirks(ps_gpu *h, int32_t quirks)
 
 extern "C" void *ps_gpu_stream(ps_gpu *h) { return h ? (void *)h->stream : nullptr; }
 
-template <typename T>
-static cudaError_t upload(DevBuf<T> &b, const std::vector<T> &v, cudaStream_t s)
-{
-    cudaError_t e = b.ensure(v.size());
-    if (e != cudaSuccess) return e;
-    return cudaMemcpyAsync(b.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
-}
 
 extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_step, double stop_condition,
                                       int32_t n_iter_min, double conw_r, double conw_r_rms, int32_t ndata,
@@ -245,18 +185,18 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
     std::vector<double> cgf(cg_first, cg_first + nc);
 
     cudaStream_t s = h->stream;
-    PSB_CUDA(upload(h->facet, facet, s));
-    PSB_CUDA(upload(h->ysh, ysh, s));
-    PSB_CUDA(upload(h->pt_a, pa, s));
-    PSB_CUDA(upload(h->pt_b, pb, s));
-    PSB_CUDA(upload(h->pt_w, pw, s));
-    PSB_CUDA(upload(h->pt_rec, prec, s));
-    PSB_CUDA(upload(h->pt_curve, pcur, s));
-    PSB_CUDA(upload(h->curve_start, cstart, s));
-    PSB_CUDA(upload(h->curve_rel, crel, s));
-    PSB_CUDA(upload(h->curve_sig, csig, s));
-    PSB_CUDA(upload(h->fidx, fidx, s));
-    PSB_CUDA(upload(h->cg_first, cgf, s));
+    PSB_CUDA(psb::upload(h->facet, facet, s));
+    PSB_CUDA(psb::upload(h->ysh, ysh, s));
+    PSB_CUDA(psb::upload(h->pt_a, pa, s));
+    PSB_CUDA(psb::upload(h->pt_b, pb, s));
+    PSB_CUDA(psb::upload(h->pt_w, pw, s));
+    PSB_CUDA(psb::upload(h->pt_rec, prec, s));
+    PSB_CUDA(psb::upload(h->pt_curve, pcur, s));
+    PSB_CUDA(psb::upload(h->curve_start, cstart, s));
+    PSB_CUDA(psb::upload(h->curve_rel, crel, s));
+    PSB_CUDA(psb::upload(h->curve_sig, csig, s));
+    PSB_CUDA(psb::upload(h->fidx, fidx, s));
+    PSB_CUDA(psb::upload(h->cg_first, cgf, s));
     PSB_CUDA(h->queue.ensure(1));
     if (!h->status.ptr) {
         PSB_CUDA(h->status.ensure(1));
@@ -308,7 +248,7 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
         n_iter_min = 0;
     }
     if (stop_condition < 1) {
-        n_iter_max = kMaxIter;
+        n_iter_max = psb::kMaxIter;
         iter_diff_max = stop_condition;
     }
     p.n_iter_max = n_iter_max;
@@ -362,7 +302,7 @@ static ps_status run_items(ps_gpu *h, const std::vector<psb::FitItem> &items, st
     const int n = (int)items.size();
     res.resize(n);
     if (n == 0) return PS_OK;
-    PSB_CUDA(upload(h->items, items, h->stream));
+    PSB_CUDA(psb::upload(h->items, items, h->stream));
     PSB_CUDA(h->out.ensure(n));
     ps_status st = enqueue_fits(h, n, h->items.ptr, h->out.ptr);
     if (st != PS_OK) return st;
@@ -455,7 +395,7 @@ extern "C" ps_status ps_gpu_status(ps_gpu *h, int32_t *flags)
 
 // Best pole of one frequency: NaN-safe, earliest pole wins ties
 // (start_CUDA.cu:1200-1229).
-static int best_pole(const psb::FitOut *r)
+int psb_best_pole(const psb::FitOut *r)
 {
     int best = -1;
     for (int p = 0; p < PS_N_POLES; ++p)
@@ -484,7 +424,7 @@ extern "C" ps_status ps_gpu_precalc(ps_gpu *h, double freq_start, double freq_en
     st = run_items(h, items, res);
     if (st != PS_OK) return st;
     double sum_dark = 0.0;
-    for (int t = 0; t < max_test_periods; ++t) sum_dark = sum_dark + res[t * PS_N_POLES + best_pole(&res[t * PS_N_POLES])].dark;
+    for (int t = 0; t < max_test_periods; ++t) sum_dark = sum_dark + res[t * PS_N_POLES + psb_best_pole(&res[t * PS_N_POLES])].dark;
     const double ave = sum_dark / max_test_periods;
     if (ave < 1.0) *new_conw = 1;
     if (ave >= 1.0) *conw_r = *conw_r * 2;
@@ -526,7 +466,7 @@ extern "C" ps_status ps_gpu_start(ps_gpu *h, int32_t n_start_from, double freq_s
         if (st != PS_OK) return st;
         for (int q = 0; q < nf; ++q) {
             const psb::FitOut *r = &res[(size_t)q * PS_N_POLES];
-            const psb::FitOut &b = r[best_pole(r)];
+            const psb::FitOut &b = r[psb_best_pole(r)];
             ps_line &L = lines[f0 + q];
             L.period_h = 24 * b.per;
             L.rms = b.dev;

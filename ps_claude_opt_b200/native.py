@@ -43,6 +43,19 @@ class FitResult(C.Structure):
                 ("niter", C.c_int32), ("status", C.c_int32)]
 
 
+class Object(C.Structure):
+    """ps_object: one object of ps_gpu_scan_batch."""
+    _fields_ = [("beta_pole", _dp), ("lambda_pole", _dp), ("par", _dp),
+                ("cl", C.c_double), ("alamda_start", C.c_double), ("alamda_incr", C.c_double),
+                ("alamda_incrr", C.c_double), ("phi0", C.c_double), ("ndata", C.c_int32),
+                ("tim", _dp), ("ee", _dp), ("ee0", _dp), ("weight", _dp), ("brightness", _dp), ("sig", _dp),
+                ("sigr2", _dp), ("ia", _ip), ("ia_par", _ip), ("cg_first", _dp), ("numfac", C.c_int32),
+                ("curves", Curves), ("shape", Shape), ("freq_start", C.c_double), ("freq_end", C.c_double),
+                ("freq_step", C.c_double), ("stop_condition", C.c_double), ("n_iter_min", C.c_int32),
+                ("escl", C.c_double), ("conw_r", C.c_double), ("n_start_from", C.c_int32),
+                ("max_lines", C.c_int32)]
+
+
 PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.c_int32)
 
 # name -> (restype, argtypes)
@@ -75,6 +88,8 @@ _SIGS = {
                                        C.c_double, C.c_int32, C.c_double, C.c_double, C.c_int32, _ip, _ip, _dp,
                                        _dp, _dp, C.c_int32, _dp, C.POINTER(Curves), C.POINTER(Shape), C.c_int32,
                                        _ip, _ip, C.POINTER(FitResult)]),
+    "ps_gpu_scan_batch": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(Object), C.c_int32, C.POINTER(Line),
+                                    C.POINTER(C.c_int64), _ip, _dp]),
     "ps_n_coef": (C.c_int32, [C.c_int32, C.c_int32]),
     "ps_measure_fp64_peak": (C.c_int, [C.c_int32, _dp]),
     "ps_probe_reciprocal": (C.c_int, [C.c_int32, _dp, _dp]),
@@ -317,6 +332,54 @@ def fit_items_noalloc(obj, n_freq, pole, device=0, conw_r=None):
     niter = np.array([r.niter for r in res[:n]], dtype=np.int32)
     status = np.array([r.status for r in res[:n]], dtype=np.int32)
     return out.reshape(n, 6), niter, status
+
+
+def scan_batch(objs, device=0, quirks=0, max_freq=None):
+    """ps_gpu_scan_batch over prepared objects: each object's convexity-weight
+    search and scan, all on one GPU at once.  Returns [(lines, conw_r)] in the
+    order of objs, as run_object gives them one by one."""
+    keep = []
+
+    def arr(x, dt=np.float64):
+        a = np.ascontiguousarray(x, dtype=dt)
+        keep.append(a)
+        return a
+
+    n = len(objs)
+    cs = (Object * max(n, 1))()
+    offs = np.zeros(max(n, 1), dtype=np.int64)
+    total = 0
+    for i, o in enumerate(objs):
+        g = o.grid
+        nl = g.n_max if max_freq is None else min(g.n_max, max_freq)
+        offs[i] = total
+        total += nl
+        c = cs[i]
+        c.beta_pole, c.lambda_pole, c.par = _p(arr(o.beta_pole)), _p(arr(o.lambda_pole)), _p(arr(o.par))
+        c.cl, c.alamda_start, c.alamda_incr, c.alamda_incrr = float(o.cl), o.alamda_start, o.alamda_incr, o.alamda_incrr
+        c.phi0, c.ndata = o.phi0, o.n_points
+        c.tim, c.ee, c.ee0, c.weight = _p(arr(o.tim)), _p(arr(o.ee)), _p(arr(o.ee0)), _p(arr(o.weight))
+        c.brightness, c.sig, c.sigr2 = _p(arr(o.brightness)), _p(arr(o.sig)), _p(arr(o.sigr2))
+        c.ia = _p(arr(o.ia, np.int32), C.c_int32)
+        c.ia_par = _p(arr(o.ia[o.n_coef + 4:o.n_coef + 7], np.int32), C.c_int32)
+        c.cg_first, c.numfac = _p(arr(o.cg_first)), o.n_fac
+        c.curves = Curves(o.n_curves, _p(arr(o.curve_len, np.int32), C.c_int32),
+                          _p(arr(o.curve_rel, np.int32), C.c_int32))
+        c.shape = Shape(o.n_coef, _p(arr(o.normal)), _p(arr(o.d_area)), _p(arr(o.dsph)))
+        c.freq_start, c.freq_end, c.freq_step = g.freq_start, g.freq_end, g.freq_step
+        c.stop_condition, c.n_iter_min = float(o.stop_condition), o.n_iter_min
+        c.escl, c.conw_r, c.n_start_from, c.max_lines = o.escl, o.conw_r, 1, nl
+    lines = (Line * max(total, 1))()
+    nl = np.zeros(max(n, 1), dtype=np.int32)
+    cw = np.zeros(max(n, 1))
+    _check(lib().ps_gpu_scan_batch(device, n, cs, quirks, lines, offs.ctypes.data_as(C.POINTER(C.c_int64)),
+                                   _p(nl, C.c_int32), _p(cw)))
+    out = []
+    for i in range(n):
+        ls = lines[int(offs[i]):int(offs[i]) + int(nl[i])]
+        out.append((np.array([(l.period_h, l.rms, l.chisq, l.dark, l.lambda_deg, l.beta_deg) for l in ls]),
+                    float(cw[i])))
+    return out
 
 
 def run_object(obj, device=0, quirks=0, max_freq=None, progress=None):

@@ -11,6 +11,9 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+    # temporary files of the tests stay inside the repository tree
+    if config.option.basetemp is None:
+        config.option.basetemp = os.path.join(ROOT, ".pytest_tmp")
 
 
 @functools.lru_cache(maxsize=None)
@@ -28,6 +31,12 @@ def synth_text(kind: str, seed: int):
         # C2 shape (lmax 6, nrows 8, 40 dense + 400 calibrated points), few frequencies
         "c2": synth.SynthConfig(l_max=6, m_max=6, nrows=8, n_dense=40, dense_pts=(50, 120), n_sparse=400,
                                 sparse_curves=2, n_freq=4),
+        # the largest model: lmax 8 (81 coefficients, ma 89), 800 facets, calibrated data
+        # (ia[1] fitted -> 88 fitted parameters: 12 x 12 blocks of J^T W J)
+        "lmax8": synth.SynthConfig(l_max=8, m_max=8, nrows=10, n_dense=4, dense_pts=(30, 40), n_sparse=40,
+                                   sparse_curves=1, n_freq=3),
+        # lmax 8, relative data only (87 fitted parameters)
+        "lmax8rel": synth.SynthConfig(l_max=8, m_max=8, nrows=10, n_dense=5, dense_pts=(30, 40), n_freq=3),
     }
     text, truth = synth.generate(cfgs[kind], seed)
     return text, truth

@@ -30,6 +30,48 @@ def test_library_exports_every_declared_symbol():
     assert set(names) <= set(native.exported_symbols())
 
 
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of the ABI structs have the C compiler's layout."""
+    import ctypes
+    import subprocess
+
+    from ps_claude_opt_b200 import native
+
+    checks = {"ps_object": native.Object, "ps_curves": native.Curves, "ps_shape": native.Shape,
+              "ps_line": native.Line, "ps_fit_result": native.FitResult}
+    lines = []
+    for cname, py in checks.items():
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"ps_b200.h\"\nint main(void) {\n" +
+                   "\n".join(lines) + "\nreturn 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    for row in filter(None, out):
+        cname, fname, val = row.split()
+        py = checks[cname]
+        want = ctypes.sizeof(py) if fname == "sizeof" else getattr(py, fname).offset
+        assert int(val) == want, (cname, fname)
+
+
+def test_scan_batch_validates_before_touching_the_gpu():
+    import ctypes
+
+    from ps_claude_opt_b200 import native
+
+    assert native.scan_batch([]) == []
+    o = (native.Object * 1)()          # n_start_from = 0 is invalid
+    lines = (native.Line * 1)()
+    off = (ctypes.c_int64 * 1)(0)
+    nl = (ctypes.c_int32 * 1)(0)
+    cw = (ctypes.c_double * 1)(0)
+    rc = native.lib().ps_gpu_scan_batch(0, 1, o, 0, lines, off, nl, cw)
+    assert rc == 1 and b"n_start_from" in native.lib().ps_last_error()
+
+
 def test_version_string():
     from ps_claude_opt_b200 import native
 
