@@ -33,6 +33,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "ps_b200.h"
 #include "ps_input.h"
 
@@ -178,6 +180,10 @@ int main(int argc, char **argv)
     const double lambda_pole[PS_N_POLES] = {0, 90, 180, 270, 60, 180, 300, 60, 180, 300};
     const double beta_pole[PS_N_POLES] = {0, 0, 0, 0, 60, 60, 60, -60, -60, -60};
 
+    // the host thread sleeps while the GPU works instead of spinning
+    // (as the reference asks for, start_CUDA.cu:129-148); the flag only
+    // takes effect before the device is first used
+    cudaSetDeviceFlags(cudaDeviceScheduleBlockingSync);
     ps_gpu *h = nullptr;
     if (ps_gpu_prepare(opt.device, beta_pole, lambda_pole, obj.par, obj.cl, obj.lambda_start, obj.lambda_incr,
                        obj.lambda_incrr, obj.ee.data(), obj.ee0.data(), obj.tim.data(), obj.phi0, obj.n_points,
