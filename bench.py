@@ -301,6 +301,32 @@ def main():
         e2e_ms.append((time.perf_counter() - t0) * 1000)
     e2e_value = n_fits * world / (np.mean(e2e_ms) / 1000.0)
 
+    # the same steps with the mixed-precision sweep (FP32 facet terms, 3xTF32
+    # tensor-core shape derivatives; FP64 elsewhere), device-timed the same way
+    eng.set_precision(native.PRECISION_MIXED)
+    eng.configure(conw_r=obj.conw_r)
+    with torch.cuda.stream(stream):
+        flush.fill_(1)
+        run_step(0)
+    torch.cuda.synchronize()
+    evm = []
+    with torch.cuda.stream(stream):
+        for s in range(args.warmup, steps_total):
+            flush.fill_(s & 0xFF)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run_step(s)
+            e1.record(stream)
+            evm.append((e0, e1))
+    torch.cuda.synchronize()
+    mixed_ms = float(sum(a.elapsed_time(b) for a, b in evm))
+    if dist:
+        t = torch.tensor([mixed_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        mixed_ms = float(t.item())
+    mixed_value = n_fits * args.steps * world / (mixed_ms / 1000.0)
+
     line = None
     if rank == 0:
         n_obj = n_max * 10
@@ -327,6 +353,10 @@ def main():
             "e2e": {"value": e2e_value, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": float(np.mean(e2e_ms))},
             "gpu_launches": args.steps,
+            "mixed": {"value": mixed_value, "unit": "fits/s", "ms_per_step": mixed_ms / args.steps,
+                      "s_per_object": n_obj / (mixed_value / world), "gpu_launches": args.steps,
+                      "precision": "facet sweep FP32 with 3xTF32 tensor-core shape derivatives; geometry, "
+                                   "J^T W J, chi^2, Gauss-Jordan and lambda update FP64"},
         }
         if world == 1 and not args.no_cpu_baseline:
             cores = os.cpu_count() or 1

@@ -188,6 +188,20 @@ ps_status ps_gpu_eval(ps_gpu *h, const double *a, double *chisq, double *alpha, 
 /* Device-status bits (PS_DEVSTAT_*) accumulated since prepare. */
 ps_status ps_gpu_status(ps_gpu *h, int32_t *flags);
 ps_status ps_gpu_set_quirks(ps_gpu *h, int32_t quirks);
+
+/* Arithmetic of the fit (no reference counterpart; the reference's own
+   reduced-precision path is its df64 FP32-pair emulation, mreal.h:65-517).
+   PS_PRECISION_FP64: FP64 throughout (default).  PS_PRECISION_MIXED: the
+   facet sweep -- brightness, its parameter derivatives and the per-point
+   sums -- runs in FP32, its shape-derivative products on the tensor cores
+   as 3xTF32 (high x high + high x low + low x high) with FP32 accumulation,
+   the per-point scalar sums flushed to FP64 every 32 facets; geometry,
+   J^T W J, chi^2, the Gauss-Jordan solve and the lambda update stay FP64.
+   For n_coef <= 64 (lmax <= 7).  Takes effect at the next configure (or
+   precalc / start, which configure). */
+#define PS_PRECISION_FP64 0
+#define PS_PRECISION_MIXED 1
+ps_status ps_gpu_set_precision(ps_gpu *h, int32_t precision);
 /* Per-phase SM clock totals of the fit kernel (diagnostics; no reference
    counterpart).  If out is non-null it receives 12 values accumulated since
    the last call -- cycles in curv, point sort, facet sweep, curve statistics,

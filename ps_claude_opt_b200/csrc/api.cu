@@ -86,7 +86,7 @@ extern "C" void ps_gpu_unprepare(ps_gpu *h)
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->facet.release(); h->pt_a.release(); h->pt_b.release(); h->pt_rec.release();
-    h->ysh.release(); h->pt_w.release(); h->curve_sig.release(); h->cg_first.release();
+    h->ysh.release(); h->ysh32.release(); h->pt_w.release(); h->curve_sig.release(); h->cg_first.release();
     h->scratch.release(); h->eval_buf.release();
     h->pt_curve.release(); h->curve_start.release(); h->curve_rel.release(); h->fidx.release();
     h->queue.release(); h->status.release(); h->items.release(); h->out.release(); h->phase.release();
@@ -102,6 +102,29 @@ extern "C" ps_status ps_gpu_set_quirks(ps_gpu *h, int32_t quirks)
 }
 
 extern "C" void *ps_gpu_stream(ps_gpu *h) { return h ? (void *)h->stream : nullptr; }
+
+extern "C" ps_status ps_gpu_set_precision(ps_gpu *h, int32_t precision)
+{
+    if (!h) return psb_fail(PS_ERR_NOT_PREPARED, "ps_gpu_set_precision: null handle");
+    if (precision != PS_PRECISION_FP64 && precision != PS_PRECISION_MIXED)
+        return psb_fail(PS_ERR_ARG, "ps_gpu_set_precision: unknown precision");
+    h->precision = precision;
+    h->configured = false;  // takes effect at the next configure
+    return PS_OK;
+}
+
+// Rounds x to the nearest TF32 value (10 explicit mantissa bits, ties to
+// even); finite inputs only.
+static float tf32_round(float x)
+{
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    const uint32_t lsb = (u >> 13) & 1u;
+    u = (u + 0x0fffu + lsb) & ~0x1fffu;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
 
 
 extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_step, double stop_condition,
@@ -141,18 +164,21 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
 
     cudaDeviceProp prop;
     PSB_CUDA(cudaGetDeviceProperties(&prop, h->device));
+    const int mixed = h->precision == PS_PRECISION_MIXED ? 1 : 0;
+    if (mixed && ncp > psb::kMaxMixedNcp)
+        return psb_fail(PS_ERR_ARG, "ps_gpu_configure: mixed precision is built for n_coef <= 64 (lmax <= 7)");
     // preferred layout first: 32-row tiles with the per-curve statistics in
     // shared memory; fall back for the largest models
     int tile_rows = 32, cstat_smem = 1;
     const int rs = (ma + 2) & ~1;
-    size_t smem = psb::fit_smem_bytes(numfac, mfit, ncp, curves->n_curves, rs, tile_rows, cstat_smem);
+    size_t smem = psb::fit_smem_bytes(numfac, mfit, ncp, curves->n_curves, rs, tile_rows, cstat_smem, mixed);
     if (smem > prop.sharedMemPerBlockOptin) {
         cstat_smem = 0;
-        smem = psb::fit_smem_bytes(numfac, mfit, ncp, curves->n_curves, rs, tile_rows, cstat_smem);
+        smem = psb::fit_smem_bytes(numfac, mfit, ncp, curves->n_curves, rs, tile_rows, cstat_smem, mixed);
     }
     if (smem > prop.sharedMemPerBlockOptin) {
         tile_rows = 16;
-        smem = psb::fit_smem_bytes(numfac, mfit, ncp, curves->n_curves, rs, tile_rows, cstat_smem);
+        smem = psb::fit_smem_bytes(numfac, mfit, ncp, curves->n_curves, rs, tile_rows, cstat_smem, mixed);
     }
     if (smem > prop.sharedMemPerBlockOptin)
         return psb_fail(PS_ERR_ARG, "ps_gpu_configure: object too large for shared memory");
@@ -164,6 +190,22 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
     std::vector<double> ysh((size_t)numfac * ncp, 0.0);
     for (int f = 0; f < numfac; ++f)
         for (int k = 0; k < nc; ++k) ysh[(size_t)f * ncp + k] = shape->d_sphere[(size_t)f * nc + k];
+    // mixed precision: the basis as TF32 high and low parts, chunk by chunk
+    // ([chunk][hi | lo][chunk facets][ncp], zero past the last facet)
+    std::vector<float> ysh32;
+    if (mixed) {
+        const int fc = psb::chunk_facets_of(ncp), nch = (numfac + fc - 1) / fc;
+        ysh32.assign((size_t)nch * 2 * fc * ncp, 0.0f);
+        for (int f = 0; f < numfac; ++f) {
+            const size_t base = (size_t)(f / fc) * 2 * fc * ncp + (size_t)(f % fc) * ncp;
+            for (int k = 0; k < nc; ++k) {
+                const double y = shape->d_sphere[(size_t)f * nc + k];
+                const float hi = tf32_round((float)y);
+                ysh32[base + k] = hi;
+                ysh32[base + (size_t)fc * ncp + k] = tf32_round((float)(y - (double)hi));
+            }
+        }
+    }
     std::vector<double4> pa(ndata), pb(ndata), prec(ndata);
     std::vector<double> pw(ndata);
     std::vector<int> pcur(ndata), cstart(curves->n_curves + 1), crel(curves->n_curves);
@@ -187,6 +229,7 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
     cudaStream_t s = h->stream;
     PSB_CUDA(psb::upload(h->facet, facet, s));
     PSB_CUDA(psb::upload(h->ysh, ysh, s));
+    if (mixed) PSB_CUDA(psb::upload(h->ysh32, ysh32, s));
     PSB_CUDA(psb::upload(h->pt_a, pa, s));
     PSB_CUDA(psb::upload(h->pt_b, pb, s));
     PSB_CUDA(psb::upload(h->pt_w, pw, s));
@@ -227,6 +270,8 @@ extern "C" ps_status ps_gpu_configure(ps_gpu *h, double freq_start, double freq_
     o.curve_sig = h->curve_sig.ptr;
     o.fidx = h->fidx.ptr;
     o.cg_first = h->cg_first.ptr;
+    o.mixed = mixed;
+    o.ysh32 = mixed ? h->ysh32.ptr : nullptr;
 
     psb::DevParams &p = h->prm;
     p.phi0 = h->phi0;

@@ -21,10 +21,13 @@ int padded_ncoef(int n_coef)
     return -1;
 }
 
-size_t fit_smem_bytes(int n_fac, int mfit, int ncp, int n_curves, int row_stride, int tile_rows, int cstat_smem)
+size_t fit_smem_bytes(int n_fac, int mfit, int ncp, int n_curves, int row_stride, int tile_rows, int cstat_smem,
+                      int mixed)
 {
-    return carve_bytes(n_fac, mfit, ncp, n_curves, row_stride, tile_rows, cstat_smem, nullptr, nullptr);
+    return carve_bytes(n_fac, mfit, ncp, n_curves, row_stride, tile_rows, cstat_smem, mixed, nullptr, nullptr);
 }
+
+int chunk_facets_of(int ncp) { return chunk_facets(ncp); }
 
 size_t fit_scratch_doubles(const DevObject &o)
 {
@@ -32,13 +35,31 @@ size_t fit_scratch_doubles(const DevObject &o)
     return (n + 31) & ~size_t(31);
 }
 
+// The mixed-precision sweep is built for the smaller bases (chunks of 32
+// facets, ncp <= kMaxMixedNcp).
+#define PSB_MIXED_LIST(X) X(16) X(24) X(32) X(40) X(48) X(56) X(64)
+
 // One translation unit per instance (fit_inst.cu) exports its kernel.
 #define PSB_DECL(N) KernelFn fit_kernel_ptr_##N();
 PSB_NCP_LIST(PSB_DECL)
 #undef PSB_DECL
+#define PSB_DECLM(N) KernelFn fit_kernel_mixed_ptr_##N();
+PSB_MIXED_LIST(PSB_DECLM)
+#undef PSB_DECLM
 
-static KernelFn kernel_for(int ncp)
+static KernelFn kernel_for(int ncp, int mixed)
 {
+    if (mixed) {
+        switch (ncp) {
+#define PSB_CASEM(N) \
+    case N:          \
+        return fit_kernel_mixed_ptr_##N();
+            PSB_MIXED_LIST(PSB_CASEM)
+#undef PSB_CASEM
+        default:
+            return nullptr;
+        }
+    }
     switch (ncp) {
 #define PSB_CASE(N) \
     case N:         \
@@ -52,9 +73,9 @@ static KernelFn kernel_for(int ncp)
 
 static int prepare_kernel(const DevObject &o, KernelFn *fn, size_t *smem)
 {
-    *fn = kernel_for(o.ncp);
+    *fn = kernel_for(o.ncp, o.mixed);
     if (!*fn) return (int)cudaErrorInvalidValue;
-    *smem = fit_smem_bytes(o.n_fac, o.mfit, o.ncp, o.n_curves, o.row_stride, o.tile_rows, o.cstat_smem);
+    *smem = fit_smem_bytes(o.n_fac, o.mfit, o.ncp, o.n_curves, o.row_stride, o.tile_rows, o.cstat_smem, o.mixed);
     cudaError_t e = cudaFuncSetAttribute(*fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem);
     return (int)e;
 }

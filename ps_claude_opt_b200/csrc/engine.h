@@ -34,6 +34,11 @@ struct DevObject {
     const double *curve_sig;  // [n_curves] mean brightness (sigma of a relative curve)
     const int *fidx;          // [mfit] 1-based index of each fitted parameter
     const double *cg_first;   // [n_coef]
+    // mixed precision (0: FP64 throughout): the facet sweep runs in FP32 with
+    // 3xTF32 tensor-core products; ysh32 holds the basis split into TF32
+    // high and low parts, chunk by chunk: [chunk][hi | lo][chunk_facets][ncp]
+    int mixed;
+    const float *ysh32;
 };
 
 struct DevParams {
@@ -73,7 +78,12 @@ enum StatusBits : int {
 };
 
 // Bytes of dynamic shared memory one fit CTA needs.
-size_t fit_smem_bytes(int n_fac, int mfit, int ncp, int n_curves, int row_stride, int tile_rows, int cstat_smem);
+size_t fit_smem_bytes(int n_fac, int mfit, int ncp, int n_curves, int row_stride, int tile_rows, int cstat_smem,
+                      int mixed);
+// Largest padded coefficient count the mixed-precision sweep is built for.
+constexpr int kMaxMixedNcp = 64;
+// Facets per basis chunk of the facet sweep for a padded coefficient count.
+int chunk_facets_of(int ncp);
 // Doubles of scratch one CTA needs (derivative rows + per-curve statistics).
 size_t fit_scratch_doubles(const DevObject &o);
 // Padded coefficient count the kernels are compiled for.

@@ -1,9 +1,13 @@
 // fit_inst.cu -- one instance of the fit kernel, compiled once per padded
-// coefficient count (-DPSB_NCP=16..88) so the instances build in parallel.
+// coefficient count (-DPSB_NCP=16..88) and precision (-DPSB_MIXED=0/1) so
+// the instances build in parallel.
 #include "fit_kernel.cuh"
 
 #ifndef PSB_NCP
 #error "compile with -DPSB_NCP=<padded coefficient count>"
+#endif
+#ifndef PSB_MIXED
+#define PSB_MIXED 0
 #endif
 
 namespace psb {
@@ -13,6 +17,10 @@ using KernelFn = void (*)(DevObject, DevParams, const FitItem *, int, int *, Fit
 
 #define PSB_CAT2(a, b) a##b
 #define PSB_CAT(a, b) PSB_CAT2(a, b)
-KernelFn PSB_CAT(fit_kernel_ptr_, PSB_NCP)() { return fit_kernel<PSB_NCP>; }
+#if PSB_MIXED
+KernelFn PSB_CAT(fit_kernel_mixed_ptr_, PSB_NCP)() { return fit_kernel<PSB_NCP, true>; }
+#else
+KernelFn PSB_CAT(fit_kernel_ptr_, PSB_NCP)() { return fit_kernel<PSB_NCP, false>; }
+#endif
 
 }  // namespace psb

@@ -47,6 +47,8 @@ enum { C_ITEM, C_NITER, C_STATUS, C_ERR, C_IROW, C_ICOL, C_GO, C_ACCEPT, C_TIMEO
 enum { T_CURV, T_SORT, T_SWEEP, T_CSTAT, T_TILES, T_PSEUDO, T_SOLVE, T_REST, T_TWAIT, T_TSTAGE, T_TSYRK,
        T_NPHASE };
 
+constexpr int kWS = 12;  // row stride (floats) of the mixed-precision weight tile: conflict-free A fragments
+
 // Facets per basis chunk: keeps kStages chunks within ~60 KB of shared memory.
 __host__ __device__ inline int chunk_facets(int ncp) { return ncp <= 64 ? 32 : 16; }
 
@@ -67,6 +69,8 @@ struct Sh {
     double *crave;    // [n_curves] 1 / sum(ymod) of each relative curve
     double *cst;      // [n_curves][ma + 3] per-curve statistics (when they fit here)
     double *wst;      // [kWarps][32][4] facet weights of one k-step, per warp (sweep MMA operand A)
+    float *wst32;     // mixed precision: [kWarps][hi | lo][32][kWS] TF32 facet weights (same storage as wst)
+    float4 *F32;      // mixed precision: [n_fac] normal + current area in FP32
     double *ybuf;     // [kStages][chunk_facets][ncp] basis chunks of the facet sweep
     unsigned long long *mbar;  // [kStages] completion barriers of the chunk copies
     long long *tclk;  // [T_NPHASE + 1] phase clocks, last slot = previous mark
@@ -174,7 +178,7 @@ __host__ __device__ inline size_t scratch_perm(int n_points, int row_stride, int
 }
 
 __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, int n_curves, int rs, int tr,
-                                              int cstat_smem, Sh *s, unsigned char *base)
+                                              int cstat_smem, int mixed, Sh *s, unsigned char *base)
 {
     int ld = fit_ld(mfit), mfp = fit_mfp(mfit);
     size_t off = 0;
@@ -218,7 +222,8 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, int 
     void *crave = take(sizeof(double) * n_curves);
     // rs = row stride = ma + 1 rounded to even, so ma + 3 <= rs + 2
     void *cst = take(cstat_smem ? sizeof(double) * n_curves * (rs + 2) : 0);
-    void *wst = take(sizeof(double) * kWarps * 32 * 4);
+    void *wst = take(mixed ? sizeof(float) * kWarps * 2 * 32 * kWS : sizeof(double) * kWarps * 32 * 4);
+    void *f32 = take(mixed ? sizeof(float4) * n_fac : 0);
     if (s) {
         s->F = (double4 *)F; s->alpha = (double *)alpha; s->covar = (double *)covar;
         s->beta = (double *)beta; s->da = (double *)da; s->a = (double *)a; s->atry = (double *)atry;
@@ -235,6 +240,8 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, int 
         s->tclk = (long long *)tclk; s->hist = (int *)hist;
         s->ccoef = (double *)ccoef; s->crave = (double *)crave; s->cst = (double *)cst;
         s->wst = (double *)wst;
+        s->wst32 = (float *)wst;
+        s->F32 = (float4 *)f32;
         s->ld = ld; s->mfp = mfp; s->tr = tr;
     }
     return off;
@@ -667,6 +674,257 @@ __device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows, c
     }
 }
 
+// ---------------------------------------------------------------- phase B, mixed precision
+
+__device__ __forceinline__ uint32_t tf32_rna(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// D += A B on the tensor cores, m16n8k8, TF32 operands, FP32 accumulation.
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// The facet sweep in mixed precision: the point geometry and the output rows
+// stay FP64; the per-facet Lambert + Lommel-Seeliger terms run in FP32 with
+// the per-point sums flushed into FP64 after every chunk of facets; the shape
+// derivatives J = W Y run on the tensor cores as 3xTF32 products
+// (W_lo Y_hi + W_hi Y_lo + W_hi Y_hi, each operand split into a TF32 high
+// part and a TF32 remainder) with FP32 accumulation.  The chunk pipeline is
+// the FP64 sweep's; a chunk holds the basis as [hi | lo][chunk_facets][ncp]
+// floats, zero-padded past the last facet.  One warp = 32 points, steps of 8
+// facets (the MMA's k); a step no lane sees is skipped whole, a 16-point half
+// that sees none of its 8 facets skips its MMAs.
+template <int NCP>
+__device__ void brightness_rows_mixed(const DevObject &o, const Sh &s, double *rows, const int *perm)
+{
+    constexpr int NT = NCP / 8;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int np = o.n_points, nf = o.n_fac, nc = o.n_coef;
+    const float cl = (float)s.inv[5], cls = (float)s.inv[6];
+    const int fc = chunk_facets(NCP);
+    const int nchunks = (nf + fc - 1) / fc;
+    const int ntiles = (np + 31) / 32;
+    const int nrounds = (ntiles + kWarps - 1) / kWarps;
+    const int total = nrounds * nchunks;
+    float *whi = s.wst32 + warp * 2 * 32 * kWS;
+    float *wlo = whi + 32 * kWS;
+    float *ybuf = reinterpret_cast<float *>(s.ybuf);
+    bool timeout = false;
+
+    auto issue = [&](int gg) {
+        const int c = gg % nchunks;
+        const int b = gg % kStages;
+        bulk_load(ybuf + (size_t)b * 2 * fc * NCP, o.ysh32 + (size_t)c * 2 * fc * NCP,
+                  (uint32_t)(2 * fc * NCP * sizeof(float)), &s.mbar[b]);
+    };
+    if (tid == 0)
+        for (int gg = 0; gg < kStages && gg < total; ++gg) issue(gg);
+
+    int gi = 0;
+    for (int round = 0; round < nrounds; ++round) {
+        const int tile = round * kWarps + warp;
+        const bool tile_act = tile < ntiles;
+        const int idx = tile * 32 + lane;
+        const bool act = tile_act && idx < np;
+        const int p = perm[min(idx, np - 1)];
+        float ex, ey, ez, sx, sy, sz;
+        {
+            const double4 pa = ldg4(&o.pt_a[p]);
+            const double4 pb = ldg4(&o.pt_b[p]);
+            const double ee[3] = {pa.y, pa.z, pa.w}, es[3] = {pb.x, pb.y, pb.z};
+            PointGeo geo;
+            point_geometry<false>(s.inv, pa.x, ee, es, geo);
+            ex = (float)geo.e[0]; ey = (float)geo.e[1]; ez = (float)geo.e[2];
+            sx = (float)geo.e0[0]; sy = (float)geo.e0[1]; sz = (float)geo.e0[2];
+        }
+
+        float C[2][NT][4];
+#pragma unroll
+        for (int m = 0; m < 2; ++m)
+#pragma unroll
+            for (int n = 0; n < NT; ++n) C[m][n][0] = C[m][n][1] = C[m][n][2] = C[m][n][3] = 0.0f;
+        // br, u0..u2, w0..w2, t4, t5 in FP64, fed by FP32 chunk partial sums
+        double S64[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+
+        for (int c = 0; c < nchunks; ++c, ++gi) {
+            const int b = gi % kStages;
+            const int use = s.ctl[C_YUSE + b] + gi / kStages;  // phase parity of this fill
+            if (!mbar_wait(&s.mbar[b], (uint32_t)(use & 1))) timeout = true;
+            if (tile_act) {
+                const int f0 = c * fc, nfc = min(fc, nf - f0);
+                const float *yh = ybuf + (size_t)b * 2 * fc * NCP;
+                const float *yl = yh + fc * NCP;
+                float S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+                for (int k0 = 0; k0 < nfc; k0 += 8) {
+                    // visibility of the step's 8 facets, one vote
+                    float mu[8], mu0[8];
+                    bool vis[8];
+                    bool v8 = false;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const bool inside = k0 + q < nfc;
+                        const float4 fr = s.F32[f0 + (inside ? k0 + q : 0)];
+                        mu[q] = ex * fr.x + ey * fr.y + ez * fr.z;
+                        mu0[q] = sx * fr.x + sy * fr.y + sz * fr.z;
+                        vis[q] = act && inside && (mu[q] > (float)kTiny) && (mu0[q] > (float)kTiny);
+                        v8 = v8 || vis[q];
+                    }
+                    const unsigned vm = __ballot_sync(0xffffffffu, v8);
+                    if (!vm) continue;  // warp-uniform
+                    uint32_t hi[8], lo[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        // lanes that do not see the facet run the same arithmetic on
+                        // finite stand-ins and contribute exact zeros
+                        const float4 fr = s.F32[f0 + (k0 + q < nfc ? k0 + q : 0)];
+                        const float ar = vis[q] ? fr.w : 0.0f;
+                        const float r = __frcp_rn(vis[q] ? mu[q] + mu0[q] : 1.0f);
+                        const float m2 = mu[q] * mu0[q];
+                        const float amm = ar * m2;
+                        const float w = amm * fmaf(cls, r, cl);
+                        const float q0 = mu0[q] * r, q1 = mu[q] * r;
+                        const float gg = ar * fmaf(cls * q0, q0, cl * mu0[q]);
+                        const float g0 = ar * fmaf(cls * q1, q1, cl * mu[q]);
+                        S[0] += w;
+                        S[1] = fmaf(gg, fr.x, S[1]);
+                        S[2] = fmaf(gg, fr.y, S[2]);
+                        S[3] = fmaf(gg, fr.z, S[3]);
+                        S[4] = fmaf(g0, fr.x, S[4]);
+                        S[5] = fmaf(g0, fr.y, S[5]);
+                        S[6] = fmaf(g0, fr.z, S[6]);
+                        S[7] += amm;
+                        S[8] = fmaf(amm, r, S[8]);
+                        hi[q] = tf32_rna(w);
+                        lo[q] = tf32_rna(w - __uint_as_float(hi[q]));
+                    }
+                    // this lane's row of the step's weight tile, high and low parts
+                    uint4 *ph = reinterpret_cast<uint4 *>(whi + lane * kWS);
+                    uint4 *pl = reinterpret_cast<uint4 *>(wlo + lane * kWS);
+                    ph[0] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+                    ph[1] = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+                    pl[0] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+                    pl[1] = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+                    __syncwarp();
+                    // A fragments: rows = points 16m + g (+8), columns = facets t (+4)
+                    uint32_t ah[2][4], al[2][4];
+#pragma unroll
+                    for (int m = 0; m < 2; ++m) {
+                        const int r0 = (16 * m + g) * kWS + t, r1 = r0 + 8 * kWS;
+                        ah[m][0] = __float_as_uint(whi[r0]);
+                        ah[m][1] = __float_as_uint(whi[r1]);
+                        ah[m][2] = __float_as_uint(whi[r0 + 4]);
+                        ah[m][3] = __float_as_uint(whi[r1 + 4]);
+                        al[m][0] = __float_as_uint(wlo[r0]);
+                        al[m][1] = __float_as_uint(wlo[r1]);
+                        al[m][2] = __float_as_uint(wlo[r0 + 4]);
+                        al[m][3] = __float_as_uint(wlo[r1 + 4]);
+                    }
+                    const bool mt0 = (vm & 0xffffu) != 0, mt1 = (vm >> 16) != 0;
+                    // B fragments: rows = facets k0 + t (+4), columns = coefficients 8n + g
+                    const float *bh = yh + (k0 + t) * NCP + g;
+                    const float *bl = yl + (k0 + t) * NCP + g;
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) {
+                        const uint32_t b0h = __float_as_uint(bh[8 * n]), b1h = __float_as_uint(bh[4 * NCP + 8 * n]);
+                        const uint32_t b0l = __float_as_uint(bl[8 * n]), b1l = __float_as_uint(bl[4 * NCP + 8 * n]);
+                        if (mt0) {
+                            mma_tf32(C[0][n], al[0], b0h, b1h);
+                            mma_tf32(C[0][n], ah[0], b0l, b1l);
+                            mma_tf32(C[0][n], ah[0], b0h, b1h);
+                        }
+                        if (mt1) {
+                            mma_tf32(C[1][n], al[1], b0h, b1h);
+                            mma_tf32(C[1][n], ah[1], b0l, b1l);
+                            mma_tf32(C[1][n], ah[1], b0h, b1h);
+                        }
+                    }
+                    __syncwarp();
+                }
+#pragma unroll
+                for (int i = 0; i < 9; ++i) S64[i] += (double)S[i];
+            }
+            // release the buffer; the last of the kWarps warps refills it
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                if (atomicAdd(&s.ctl[C_REL + b], 1) == kWarps - 1) {
+                    s.ctl[C_REL + b] = 0;
+                    if (gi + kStages < total) issue(gi + kStages);
+                }
+            }
+        }
+
+        if (tile_act) {
+            const double4 pa = ldg4(&o.pt_a[p]);
+            const double4 pb = ldg4(&o.pt_b[p]);
+            const double ee[3] = {pa.y, pa.z, pa.w}, es[3] = {pb.x, pb.y, pb.z};
+            PointGeo geo;
+            point_geometry<true>(s.inv, pa.x, ee, es, geo);
+            const double br = S64[0], u0 = S64[1], u1 = S64[2], u2 = S64[3];
+            const double w0 = S64[4], w1 = S64[5], w2 = S64[6], t4 = S64[7], t5 = S64[8];
+            const double t1 = (geo.db[0] * u0 + geo.db[1] * u1 + geo.db[2] * u2) +
+                              (geo.d0b[0] * w0 + geo.d0b[1] * w1 + geo.d0b[2] * w2);
+            const double t2 = (geo.dl[0] * u0 + geo.dl[1] * u1 + geo.dl[2] * u2) +
+                              (geo.d0l[0] * w0 + geo.d0l[1] * w1 + geo.d0l[2] * w2);
+            const double t3 = (geo.dw[0] * u0 + geo.dw[1] * u1) + (geo.d0w[0] * w0 + geo.d0w[1] * w1);
+            const double scale = geo.scale;
+            if (act) {
+                double *row = rows + (size_t)p * o.row_stride;
+                row[nc + 0] = scale * t1;
+                row[nc + 1] = scale * t2;
+                row[nc + 2] = scale * t3;
+                row[nc + 3] = br * geo.ff;
+                row[nc + 4] = br * geo.d2;
+                row[nc + 5] = br * geo.alph;
+                row[nc + 6] = scale * t4 * s.inv[5];
+                row[nc + 7] = scale * t5;
+                row[nc + 8] = br * scale;
+            }
+            // shape columns from the accumulators: element (m, n, e) of this lane
+            // is point 16m + g (+8 for e >= 2), coefficient 8n + 2t + (e & 1)
+#pragma unroll
+            for (int m = 0; m < 2; ++m)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int src = 16 * m + g + 8 * h;
+                    const int pm = __shfl_sync(0xffffffffu, p, src);
+                    const double sm = __shfl_sync(0xffffffffu, scale, src);
+                    const bool am = __shfl_sync(0xffffffffu, act ? 1 : 0, src) != 0;
+                    if (!am) continue;
+                    double *row = rows + (size_t)pm * o.row_stride;
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) {
+                        const int k = 8 * n + 2 * t;
+                        const double v0 = sm * (double)C[m][n][2 * h], v1 = sm * (double)C[m][n][2 * h + 1];
+                        if (k + 1 < nc)
+                            *reinterpret_cast<double2 *>(row + k) = make_double2(v0, v1);
+                        else if (k < nc)
+                            row[k] = v0;
+                    }
+                }
+        }
+    }
+    if (timeout) s.ctl[C_TIMEOUT] = 1;
+    __syncthreads();
+    // per-buffer fill counts carry the mbarrier phases into the next evaluation
+    if (tid == 0) {
+        for (int b = 0; b < kStages; ++b) {
+            const int uses_b = (total > b) ? (total - b + kStages - 1) / kStages : 0;
+            s.ctl[C_YUSE + b] += uses_b;
+        }
+    }
+}
+
 // ---------------------------------------------------------------- phases C, D
 
 // J^T W J, J^T W dy and chi^2 as one symmetric rank-k update of the augmented
@@ -815,7 +1073,7 @@ __device__ __forceinline__ void syrk_store(const Sh &s, int mfit, const SyrkAcc 
 // One full evaluation (mrqcof) at parameter vector a in shared memory.
 // Writes alpha (symmetric, stride ld) to dst, beta to dvec; returns chi^2 to
 // every thread.
-template <int NCP>
+template <int NCP, bool MIXED>
 __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, const double *a,
                            double *dst, double *dvec, double *rows, double *cstat, int *perm, double conw_r)
 {
@@ -826,12 +1084,20 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
     tmark(p, s, T_REST);
     double area_sum = shape_areas(o, s, a);
     if (tid == 0) s.scal[S_AREA] = area_sum;
+    if constexpr (MIXED)  // each thread converts the facets it just updated
+        for (int f = tid; f < o.n_fac; f += kThreads) {
+            const double4 fr = s.F[f];
+            s.F32[f] = make_float4((float)fr.x, (float)fr.y, (float)fr.z, (float)fr.w);
+        }
     set_invariants(o, p, s, a);
     tmark(p, s, T_CURV);
 
     sort_points(o, s, perm, perm + o.n_points);
     tmark(p, s, T_SORT);
-    brightness_rows<NCP>(o, s, rows, perm);
+    if constexpr (MIXED)
+        brightness_rows_mixed<NCP>(o, s, rows, perm);
+    else
+        brightness_rows<NCP>(o, s, rows, perm);
     // the tile phase reads the rows back through the bulk-copy (async) proxy
     asm volatile("fence.proxy.async.global;" ::: "memory");
     __syncthreads();
@@ -1228,14 +1494,15 @@ static __device__ int gauss_jordan(const Sh &s, int n)
 
 // ---------------------------------------------------------------- kernel
 
-template <int NCP>
+template <int NCP, bool MIXED>
 __global__ void __launch_bounds__(kThreads, 1)
 fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *queue, FitOut *out,
            double *scratch, size_t scratch_per_cta, int *status, EvalOut ev, int mode)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Sh s;
-    carve_bytes(o.n_fac, o.mfit, o.ncp, o.n_curves, o.row_stride, o.tile_rows, o.cstat_smem, &s, smem_raw);
+    carve_bytes(o.n_fac, o.mfit, o.ncp, o.n_curves, o.row_stride, o.tile_rows, o.cstat_smem, MIXED ? 1 : 0, &s,
+                smem_raw);
     const int tid = threadIdx.x;
     const int nc = o.n_coef, ma = o.ma, mfit = o.mfit, ld = s.ld;
     double *rows = scratch + (size_t)blockIdx.x * scratch_per_cta;
@@ -1264,7 +1531,7 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
     if (mode == 1) {  // one stand-alone evaluation (parity hook)
         for (int q = tid; q <= ma; q += kThreads) s.a[q] = ev.a[q];
         __syncthreads();
-        double chisq = evaluate<NCP>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, perm, p.conw_r);
+        double chisq = evaluate<NCP, MIXED>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, perm, p.conw_r);
         for (int idx = tid; idx < mfit * mfit; idx += kThreads) {
             const int j = idx / mfit, k = idx - j * mfit;
             ev.alpha[idx] = s.alpha[j * ld + k];
@@ -1321,7 +1588,7 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
             __syncthreads();
             if (first) {
                 if (tid == 0) s.scal[S_ALAMDA] = p.alamda_start;
-                double oc = evaluate<NCP>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, perm, p.conw_r);
+                double oc = evaluate<NCP, MIXED>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, perm, p.conw_r);
                 if (tid == 0) s.scal[S_OCHISQ] = oc;
                 for (int q = tid; q <= ma; q += kThreads) s.atry[q] = s.a[q];
                 __syncthreads();
@@ -1343,7 +1610,7 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
                 if (err == 2 && tid == 0) s.ctl[C_STATUS] |= kStatusSingular;
             }
             __syncthreads();
-            const double chisq = evaluate<NCP>(o, p, s, s.atry, s.covar, s.da, rows, cstat, perm, p.conw_r);
+            const double chisq = evaluate<NCP, MIXED>(o, p, s, s.atry, s.covar, s.da, rows, cstat, perm, p.conw_r);
             // accept / reject (mrqmin_2_end, Start.cu:300-392)
             const bool accept = chisq < s.scal[S_OCHISQ];
             __syncthreads();

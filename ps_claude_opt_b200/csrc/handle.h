@@ -58,6 +58,7 @@ struct ps_gpu {
     int n_sm = 0;
     cudaStream_t stream = nullptr;
     int quirks = 0;
+    int precision = PS_PRECISION_FP64;  // applies from the next configure
     // prepare-time inputs
     int ndata = 0;
     std::vector<double> tim, ee, ee0, weight;
@@ -70,6 +71,7 @@ struct ps_gpu {
     int ctas_per_sm = 0;
     psb::DevBuf<double4> facet, pt_a, pt_b, pt_rec;
     psb::DevBuf<double> ysh, pt_w, curve_sig, cg_first, scratch, eval_buf;
+    psb::DevBuf<float> ysh32;
     psb::DevBuf<int> pt_curve, curve_start, curve_rel, fidx, queue, status;
     psb::DevBuf<psb::FitItem> items;
     psb::DevBuf<unsigned long long> phase;

@@ -149,14 +149,14 @@ extern "C" ps_status ps_fit_items_noalloc(
     NA_CUDA(cudaGetDeviceProperties(&prop, device));
     int tile_rows = 32, cstat_smem = 1;
     const int rs = (ma + 2) & ~1;
-    size_t smem = psb::fit_smem_bytes(nfac, mfit, ncp, ncur, rs, tile_rows, cstat_smem);
+    size_t smem = psb::fit_smem_bytes(nfac, mfit, ncp, ncur, rs, tile_rows, cstat_smem, 0);
     if (smem > prop.sharedMemPerBlockOptin) {
         cstat_smem = 0;
-        smem = psb::fit_smem_bytes(nfac, mfit, ncp, ncur, rs, tile_rows, cstat_smem);
+        smem = psb::fit_smem_bytes(nfac, mfit, ncp, ncur, rs, tile_rows, cstat_smem, 0);
     }
     if (smem > prop.sharedMemPerBlockOptin) {
         tile_rows = 16;
-        smem = psb::fit_smem_bytes(nfac, mfit, ncp, ncur, rs, tile_rows, cstat_smem);
+        smem = psb::fit_smem_bytes(nfac, mfit, ncp, ncur, rs, tile_rows, cstat_smem, 0);
     }
     if (smem > prop.sharedMemPerBlockOptin)
         return psb_fail(PS_ERR_ARG, "ps_fit_items_noalloc: object too large for shared memory");

@@ -17,6 +17,8 @@ HOST_PROGRAM = os.path.join(HERE, "_lib", "period_search")
 
 N_POLES = 10
 QUIRK_PRECALC_CONW = 1
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
 DEVSTAT_SINGULAR = 1
 DEVSTAT_NAN_CHISQ = 2
 
@@ -90,6 +92,7 @@ _SIGS = {
                                        _ip, _ip, C.POINTER(FitResult)]),
     "ps_gpu_scan_batch": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(Object), C.c_int32, C.POINTER(Line),
                                     C.POINTER(C.c_int64), _ip, _dp]),
+    "ps_gpu_set_precision": (C.c_int, [C.c_void_p, C.c_int32]),
     "ps_n_coef": (C.c_int32, [C.c_int32, C.c_int32]),
     "ps_measure_fp64_peak": (C.c_int, [C.c_int32, _dp]),
     "ps_probe_reciprocal": (C.c_int, [C.c_int32, _dp, _dp]),
@@ -208,6 +211,10 @@ class Engine:
 
     def set_quirks(self, q):
         _check(lib().ps_gpu_set_quirks(self.h, q))
+
+    def set_precision(self, precision):
+        """PRECISION_FP64 or PRECISION_MIXED; applies from the next configure."""
+        _check(lib().ps_gpu_set_precision(self.h, precision))
 
     def configure(self, conw_r=None, conw_r_rms=None, stop_condition=None, grid=None):
         o = self.obj
@@ -382,11 +389,12 @@ def scan_batch(objs, device=0, quirks=0, max_freq=None):
     return out
 
 
-def run_object(obj, device=0, quirks=0, max_freq=None, progress=None):
+def run_object(obj, device=0, quirks=0, max_freq=None, progress=None, precision=PRECISION_FP64):
     """The reference's main flow after parsing: conw precalc loop, then the scan.
     Returns (lines, final conw_r)."""
     with Engine(obj, device) as eng:
         eng.set_quirks(quirks)
+        eng.set_precision(precision)
         conw_r = obj.conw_r
         new_conw = 0
         while new_conw != 1 and conw_r * obj.escl * obj.escl < 10.0:
