@@ -71,6 +71,7 @@ struct Sh {
     double *wst;      // [kWarps][32][4] facet weights of one k-step, per warp (sweep MMA operand A)
     float *wst32;     // mixed precision: [kWarps][hi | lo][32][kWS] TF32 facet weights (same storage as wst)
     float4 *F32;      // mixed precision: [n_fac] normal + current area in FP32
+    float2 *G32;      // mixed precision: [n_fac] area x Lambert weight, area x Lommel-Seeliger weight
     double *ybuf;     // [kStages][chunk_facets][ncp] basis chunks of the facet sweep
     unsigned long long *mbar;  // [kStages] completion barriers of the chunk copies
     long long *tclk;  // [T_NPHASE + 1] phase clocks, last slot = previous mark
@@ -224,6 +225,7 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, int 
     void *cst = take(cstat_smem ? sizeof(double) * n_curves * (rs + 2) : 0);
     void *wst = take(mixed ? sizeof(float) * kWarps * 2 * 32 * kWS : sizeof(double) * kWarps * 32 * 4);
     void *f32 = take(mixed ? sizeof(float4) * n_fac : 0);
+    void *g32 = take(mixed ? sizeof(float2) * n_fac : 0);
     if (s) {
         s->F = (double4 *)F; s->alpha = (double *)alpha; s->covar = (double *)covar;
         s->beta = (double *)beta; s->da = (double *)da; s->a = (double *)a; s->atry = (double *)atry;
@@ -242,6 +244,7 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, int 
         s->wst = (double *)wst;
         s->wst32 = (float *)wst;
         s->F32 = (float4 *)f32;
+        s->G32 = (float2 *)g32;
         s->ld = ld; s->mfp = mfp; s->tr = tr;
     }
     return off;
@@ -683,6 +686,14 @@ __device__ __forceinline__ uint32_t tf32_rna(float x)
     return r;
 }
 
+// Approximate FP32 reciprocal (the special-function unit's, no refinement).
+__device__ __forceinline__ float rcp_approx_f32(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // D += A B on the tensor cores, m16n8k8, TF32 operands, FP32 accumulation.
 __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
 {
@@ -784,17 +795,22 @@ __device__ void brightness_rows_mixed(const DevObject &o, const Sh &s, double *r
                     uint32_t hi[8], lo[8];
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
-                        // lanes that do not see the facet run the same arithmetic on
-                        // finite stand-ins and contribute exact zeros
-                        const float4 fr = s.F32[f0 + (k0 + q < nfc ? k0 + q : 0)];
-                        const float ar = vis[q] ? fr.w : 0.0f;
-                        const float r = __frcp_rn(vis[q] ? mu[q] + mu0[q] : 1.0f);
-                        const float m2 = mu[q] * mu0[q];
-                        const float amm = ar * m2;
-                        const float w = amm * fmaf(cls, r, cl);
-                        const float q0 = mu0[q] * r, q1 = mu[q] * r;
-                        const float gg = ar * fmaf(cls * q0, q0, cl * mu0[q]);
-                        const float g0 = ar * fmaf(cls * q1, q1, cl * mu[q]);
+                        // lanes that do not see the facet take mu = mu0 = 0, which zeroes
+                        // every term they add; with a = area, L = a cl, S = a cls and
+                        // r = 1 / (mu + mu0):
+                        //   w  = a mu mu0 (cl + cls r)            (brightness term)
+                        //   gg = mu0 (S mu0 r^2 + L) = a dS/dmu,  g0 = mu (S mu r^2 + L)
+                        const int fq = f0 + (k0 + q < nfc ? k0 + q : 0);
+                        const float4 fr = s.F32[fq];
+                        const float2 ls = s.G32[fq];
+                        const float mv = vis[q] ? mu[q] : 0.0f, m0v = vis[q] ? mu0[q] : 0.0f;
+                        const float r = rcp_approx_f32(vis[q] ? mu[q] + mu0[q] : 1.0f);
+                        const float z = fr.w * (mv * m0v);
+                        const float zr = z * r;
+                        const float w = fmaf(cls, zr, cl * z);
+                        const float y = ls.y * r;
+                        const float gg = m0v * fmaf(y * m0v, r, ls.x);
+                        const float g0 = mv * fmaf(y * mv, r, ls.x);
                         S[0] += w;
                         S[1] = fmaf(gg, fr.x, S[1]);
                         S[2] = fmaf(gg, fr.y, S[2]);
@@ -802,8 +818,8 @@ __device__ void brightness_rows_mixed(const DevObject &o, const Sh &s, double *r
                         S[4] = fmaf(g0, fr.x, S[4]);
                         S[5] = fmaf(g0, fr.y, S[5]);
                         S[6] = fmaf(g0, fr.z, S[6]);
-                        S[7] += amm;
-                        S[8] = fmaf(amm, r, S[8]);
+                        S[7] += z;
+                        S[8] += zr;
                         hi[q] = tf32_rna(w);
                         lo[q] = tf32_rna(w - __uint_as_float(hi[q]));
                     }
@@ -1084,12 +1100,16 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
     tmark(p, s, T_REST);
     double area_sum = shape_areas(o, s, a);
     if (tid == 0) s.scal[S_AREA] = area_sum;
-    if constexpr (MIXED)  // each thread converts the facets it just updated
+    set_invariants(o, p, s, a);
+    if constexpr (MIXED) {  // FP32 facet tables of the mixed-precision sweep
+        const double cl = s.inv[5], cls = s.inv[6];
         for (int f = tid; f < o.n_fac; f += kThreads) {
             const double4 fr = s.F[f];
             s.F32[f] = make_float4((float)fr.x, (float)fr.y, (float)fr.z, (float)fr.w);
+            s.G32[f] = make_float2((float)(fr.w * cl), (float)(fr.w * cls));
         }
-    set_invariants(o, p, s, a);
+        __syncthreads();
+    }
     tmark(p, s, T_CURV);
 
     sort_points(o, s, perm, perm + o.n_points);
