@@ -157,13 +157,15 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def profile_case():
+def profile_case(mixed=False):
     """One launch to capture under ncu: the production object, one fit per
-    resident CTA (1 GPU)."""
+    resident CTA (1 GPU), FP64 or mixed precision."""
     from ps_claude_opt_b200 import native
 
     obj, _ = workload()
     with native.Engine(obj, device=0) as eng:
+        if mixed:
+            eng.set_precision(native.PRECISION_MIXED)
         eng.configure(conw_r=obj.conw_r)
         ctas, nsm = eng.occupancy()
         n = ctas * nsm
@@ -186,6 +188,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="two fit-kernel launches (warm-up + one to capture), one fit per resident CTA")
+    ap.add_argument("--mixed", action="store_true", help="with --profile-case: the mixed-precision kernel")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -195,7 +198,7 @@ def main():
         return
 
     if args.profile_case:
-        profile_case()
+        profile_case(args.mixed)
         return
 
     import torch

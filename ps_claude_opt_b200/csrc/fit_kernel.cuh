@@ -7,13 +7,15 @@
 //
 //   A  curv: facet areas exp(sum a_k Y_k) into shared memory  (Start.cu:421-528)
 //   B  brightness rows: a warp takes 32 points (lane = point) and sweeps every
-//      facet once; visibility, Lambert+Lommel-Seeliger terms, and the shape
-//      derivative sum_f w_f Y_k(f) accumulate in registers.  The rotation
-//      derivatives use dT/dq . (sum_f ar dS/dmu n_f), i.e. 6 accumulators per
-//      point instead of 6 dot products per facet.  Rows go to HBM scratch.
+//      facet once; visibility and the Lambert+Lommel-Seeliger terms per lane,
+//      the shape derivatives sum_f w_f Y_k(f) as a GEMM on the FP64 tensor
+//      cores (mma.sync m8n8k4).  The rotation derivatives use
+//      dT/dq . (sum_f ar dS/dmu n_f), i.e. 6 accumulators per point instead of
+//      6 dot products per facet.  Rows go to HBM scratch.
 //   C  per relative curve: column sums and 1/sum(ymod)  (Start.cu:2519-2533)
-//   D  J^T W J, J^T W dy, chi^2: 32-row tiles staged renormalised in shared
-//      memory, alpha held in registers as 2x2 blocks owned by threads.
+//   D  J^T W J, J^T W dy, chi^2: one rank-k update of the augmented matrix
+//      [J | dy] on the FP64 tensor cores, tiles of rows bulk-copied into
+//      shared memory and renormalised on the fly.
 //
 // The LM step (damped Gauss-Jordan with full pivoting, accept/reject, lambda
 // update, rms and convergence test) follows Start.cu:300-392, 2838-3021,
@@ -28,7 +30,6 @@ namespace psb {
 
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kTiny = 1e-8;
-constexpr int kBPT = 5;  // 2x2 alpha blocks per thread: ceil(45*46/2 / 256)
 constexpr int kStages = 4;          // basis chunks in flight in the facet sweep
 constexpr int kSortBands = 8;       // point sort: bands in cos(theta) ...
 constexpr int kSortSectors = 32;    // ... x sectors in longitude of the Sun-observer bisector
@@ -1127,11 +1128,26 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
     for (int c = warp; c < o.n_curves; c += kWarps) {
         if (!o.curve_rel[c]) continue;
         const int p0 = o.curve_start[c], p1 = o.curve_start[c + 1];
-        for (int col = lane; col <= ma; col += 32) {
-            double sum = 0;
-            for (int q = p0; q < p1; ++q) sum += rows[(size_t)q * RS + col];
-            cstat[(size_t)c * CS + col] = sum;
+        // columns lane, lane + 32, lane + 64 (ma + 1 <= 90); the rows come from
+        // HBM, so each step issues the loads of 8 points before adding them
+        double sum[3] = {0, 0, 0};
+        for (int q0 = p0; q0 < p1; q0 += 8) {
+            double v[8][3];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const bool ok = q0 + u < p1;
+                const double *r = rows + (size_t)(ok ? q0 + u : p0) * RS;
+#pragma unroll
+                for (int j = 0; j < 3; ++j) v[u][j] = (ok && lane + 32 * j <= ma) ? r[lane + 32 * j] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) sum[j] += v[u][j];
         }
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            if (lane + 32 * j <= ma) cstat[(size_t)c * CS + lane + 32 * j] = sum[j];
         __syncwarp();
         if (lane == 0) {
             const double rave = 1.0 / cstat[(size_t)c * CS + ma];
