@@ -39,7 +39,8 @@ L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # `bench.py --profile-case` (the derivative-row scratch round trip; it grows
 # with the number of fits, so a launch's traffic is this times its fits).
 NCU_DRAM_BYTES_PER_FIT = 27.53e9 / 148
-METRIC = "LM fits/s (FP64 full scan of the production object, 1 B200)"
+METRIC = ("LM fits/s of the plain FP64 full scan of the production object on 1 B200 (s/object of it and of "
+          "the screened+mixed scan in the same line)")
 
 
 def workload():
@@ -330,6 +331,21 @@ def main():
         mixed_ms = float(t.item())
     mixed_value = n_fits * args.steps * world / (mixed_ms / 1000.0)
 
+    # the screened + mixed scan of the whole object, end to end on this GPU:
+    # features of all trial frequencies, the network's ranking, the mixed
+    # fits of the chosen frequencies (all 10 poles) -- the convexity-weight
+    # search, the same for both kinds of scan, is left out of both
+    from ps_claude_opt_b200 import screen
+
+    net = screen.load_model()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pred = net.predict(screen.normalise(screen.features(obj, screen.frequencies(obj), local_rank)))
+    sel = screen.select(pred) + 1
+    t_rank = time.perf_counter() - t0
+    eng.fit_items(np.repeat(sel, 10), np.tile(np.arange(10), len(sel)))
+    screened_s = time.perf_counter() - t0
+
     line = None
     if rank == 0:
         n_obj = n_max * 10
@@ -356,6 +372,12 @@ def main():
             "e2e": {"value": e2e_value, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": float(np.mean(e2e_ms))},
             "gpu_launches": args.steps,
+            "screened_mixed": {"s_per_object": screened_s, "ranking_s": t_rank, "fitted_frequencies": int(len(sel)),
+                               "n_frequencies": int(n_max), "fits": int(10 * len(sel)),
+                               "vs_plain_fp64_full_scan_s": n_obj / (value / world),
+                               "note": "top 3.4 % of the network's ranking with one neighbour each side plus a "
+                                       "2 % random audit; mixed-precision fits; trained network from "
+                                       "ps_claude_opt_b200/screen_model.npz"},
             "mixed": {"value": mixed_value, "unit": "fits/s", "ms_per_step": mixed_ms / args.steps,
                       "s_per_object": n_obj / (mixed_value / world), "gpu_launches": args.steps,
                       "precision": "facet sweep FP32 with 3xTF32 tensor-core shape derivatives; geometry, "

@@ -244,6 +244,41 @@ ps_status ps_fit_items_noalloc(int32_t device, void *stream, const double *beta_
                                const ps_curves *curves, const ps_shape *shape, int32_t n,
                                const int32_t *n_freq, const int32_t *pole, ps_fit_result *out);
 
+/* ---- learned frequency screening (no counterpart in the reference, which
+        fits every trial frequency) ---- */
+
+/* Phase-folded lightcurve features of n_freq trial frequencies (1/day: 24
+   times the grid's 1/hour), 88 per frequency: features[f*88 + 8*s + a] for
+   statistic s of the 8 per-curve statistics (phase-dispersion ratios for 64,
+   32, 16, 8 bins; shares of harmonics 1..4 in the 32-bin mean curve) and
+   aggregate a over the curves (point-weighted mean, mean, std, min,
+   25/50/75 % quantiles, max); features[f*88 + 64 + 8*k + s], the same 8
+   statistics of fold k of all points together (k = 0 all, 1 before and 2
+   after the middle of the time span).  Host arrays; at most 256
+   lightcurves. */
+ps_status ps_screen_features(int32_t device, int32_t n_points, const double *tim,
+                             const double *brightness, const ps_curves *curves, int32_t n_freq,
+                             const double *freqs, float *features);
+
+/* Device-pointer kernels of the screening network (BF16 operands, FP32
+   accumulation on the tensor cores).  ps_gemm_bf16: C[m][n] (+)= sum_k
+   A[m*sam + k*sak] B[k*sbk + n*sbn] (+ bias[n]) (ReLU if relu), written to
+   the FP32 C (row stride ldc) and/or the BF16 Cb (row stride ldcb). */
+ps_status ps_gemm_bf16(int32_t M, int32_t N, int32_t K, const void *A, int64_t sam, int64_t sak,
+                       const void *B, int64_t sbk, int64_t sbn, float *C, int32_t ldc,
+                       int32_t accumulate, const float *bias, int32_t relu, void *Cb, int32_t ldcb,
+                       void *stream);
+/* dz = dh where z > 0, else 0 (FP32 dz and/or BF16 dzb). */
+ps_status ps_relu_backward(int64_t n, const float *dh, const float *z, float *dz, void *dzb,
+                           void *stream);
+/* out[c] = sum over rows r of x[r*cols + c]. */
+ps_status ps_column_sum(int32_t rows, int32_t cols, const float *x, float *out, void *stream);
+/* One Adam step on FP32 weights w (bias-corrected with step >= 1); wb, if
+   not null, receives the BF16 copy. */
+ps_status ps_adam_step(int64_t n, float *w, const float *grad, float *m, float *v, float lr,
+                       float beta1, float beta2, float eps, int32_t step, void *wb, void *stream);
+ps_status ps_to_bf16(int64_t n, const float *x, void *y, void *stream);
+
 /* Host shape setup (trifac.c, areanorm.c, sphfunc.c, ellfit.c of the
    reference): facet normals, areas, Laplace basis and the ellipsoid fit. */
 ps_status ps_setup_shape(int32_t l_max, int32_t m_max, int32_t nrows, double a, double b, double c,

@@ -93,6 +93,16 @@ _SIGS = {
     "ps_gpu_scan_batch": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(Object), C.c_int32, C.POINTER(Line),
                                     C.POINTER(C.c_int64), _ip, _dp]),
     "ps_gpu_set_precision": (C.c_int, [C.c_void_p, C.c_int32]),
+    "ps_screen_features": (C.c_int, [C.c_int32, C.c_int32, _dp, _dp, C.POINTER(Curves), C.c_int32, _dp,
+                                     C.POINTER(C.c_float)]),
+    "ps_gemm_bf16": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
+                               C.c_int64, C.c_int64, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32,
+                               C.c_void_p, C.c_int32, C.c_void_p]),
+    "ps_relu_backward": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ps_column_sum": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ps_adam_step": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                               C.c_float, C.c_float, C.c_int32, C.c_void_p, C.c_void_p]),
+    "ps_to_bf16": (C.c_int, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ps_n_coef": (C.c_int32, [C.c_int32, C.c_int32]),
     "ps_measure_fp64_peak": (C.c_int, [C.c_int32, _dp]),
     "ps_probe_reciprocal": (C.c_int, [C.c_int32, _dp, _dp]),

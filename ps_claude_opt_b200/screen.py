@@ -1,0 +1,247 @@
+"""Learned frequency screening: rank an object's trial frequencies by the chi^2
+a small BF16 network predicts from phase-folded lightcurve features, fit the
+top-ranked share plus a random audit sample with the plain LM, and keep the
+best line of what was fitted.
+
+No counterpart in the reference, which fits every trial frequency; the full
+scan (native.run_object) stays the fallback and the judge of the screen.
+All device work runs in the library's own kernels (csrc/screen.cu): the
+feature kernel, BF16 tensor-core GEMMs, the ReLU backward, column sums and
+Adam.  PyTorch only holds the device buffers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import native
+
+import os
+
+MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "screen_model.npz")
+N_FEATURES = 88
+SIZES = (N_FEATURES, 256, 256, 256, 1)   # features -> 3 x 256 hidden -> predicted log rms
+
+
+def _lib():
+    return native.lib()
+
+
+def frequencies(obj, n_start=1, n=None):
+    """Trial frequencies of the object's grid, 1/hour (the reference's unit)."""
+    g = obj.grid
+    n = g.n_max - n_start + 1 if n is None else n
+    return g.freq_start - (np.arange(n_start, n_start + n) - 1) * g.freq_step
+
+
+def features(obj, freqs, device=0):
+    """[len(freqs), 88] float32 features of trial frequencies given in 1/hour
+    (the lightcurve times are in days: the kernel folds at 24 f)."""
+    freqs = np.ascontiguousarray(24.0 * np.asarray(freqs, dtype=np.float64))
+    out = np.zeros((len(freqs), N_FEATURES), dtype=np.float32)
+    tim = np.ascontiguousarray(obj.tim, dtype=np.float64)
+    br = np.ascontiguousarray(obj.brightness, dtype=np.float64)
+    cl = np.ascontiguousarray(obj.curve_len, dtype=np.int32)
+    cr = np.ascontiguousarray(obj.curve_rel, dtype=np.int32)
+    curves = native.Curves(len(cl), cl.ctypes.data_as(C.POINTER(C.c_int32)), cr.ctypes.data_as(C.POINTER(C.c_int32)))
+    native._check(_lib().ps_screen_features(device, len(tim), tim.ctypes.data_as(C.POINTER(C.c_double)),
+                                            br.ctypes.data_as(C.POINTER(C.c_double)), C.byref(curves), len(freqs),
+                                            freqs.ctypes.data_as(C.POINTER(C.c_double)),
+                                            out.ctypes.data_as(C.POINTER(C.c_float))))
+    return out
+
+
+def normalise(feat):
+    """Per-object standardisation of each feature over the object's
+    frequencies: the network ranks frequencies within one object."""
+    mu = feat.mean(0)
+    sd = feat.std(0)
+    return ((feat - mu) / np.where(sd > 1e-6, sd, 1.0)).astype(np.float32)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Mlp:
+    """The screening network on the device: BF16 weights and activations for
+    the tensor cores, FP32 master weights, Adam moments and gradients."""
+
+    def __init__(self, sizes=SIZES, seed=0, device="cuda"):
+        import torch
+
+        self.torch = torch
+        self.sizes = tuple(sizes)
+        self.device = device
+        rng = np.random.default_rng(seed)
+        self.W, self.b, self.Wb = [], [], []
+        for k, n in zip(self.sizes[:-1], self.sizes[1:]):
+            w = rng.standard_normal((n, k)).astype(np.float32) * np.float32(np.sqrt(2.0 / k))
+            self.W.append(torch.from_numpy(w).to(device))
+            self.b.append(torch.zeros(n, dtype=torch.float32, device=device))
+            self.Wb.append(torch.empty((n, k), dtype=torch.bfloat16, device=device))
+        self.mW = [torch.zeros_like(w) for w in self.W]
+        self.vW = [torch.zeros_like(w) for w in self.W]
+        self.mb = [torch.zeros_like(b) for b in self.b]
+        self.vb = [torch.zeros_like(b) for b in self.b]
+        self.steps = 0
+        self._sync_bf16()
+
+    def _stream(self):
+        return C.c_void_p(self.torch.cuda.current_stream().cuda_stream)
+
+    def _sync_bf16(self):
+        for w, wb in zip(self.W, self.Wb):
+            native._check(_lib().ps_to_bf16(w.numel(), _ptr(w), _ptr(wb), self._stream()))
+
+    def forward(self, xb):
+        """xb: [B, N_FEATURES] bfloat16 on the device.  Returns predictions [B] (FP32)
+        and keeps the activations for backward."""
+        torch = self.torch
+        if xb.dim() != 2 or xb.shape[1] != self.sizes[0] or xb.dtype != torch.bfloat16 or not xb.is_contiguous():
+            raise ValueError("Mlp.forward: input must be a contiguous [B, %d] bfloat16 tensor" % self.sizes[0])
+        B = xb.shape[0]
+        self.hb, self.hf = [xb], [None]
+        L = len(self.W)
+        for l in range(L):
+            n, k = self.W[l].shape
+            last = l == L - 1
+            hf = torch.empty((B, n), dtype=torch.float32, device=self.device)
+            hb = None if last else torch.empty((B, n), dtype=torch.bfloat16, device=self.device)
+            native._check(_lib().ps_gemm_bf16(B, n, k, _ptr(self.hb[-1]), k, 1, _ptr(self.Wb[l]), 1, k, _ptr(hf), n,
+                                              0, _ptr(self.b[l]), 0 if last else 1, _ptr(hb), n, self._stream()))
+            self.hf.append(hf)
+            self.hb.append(hb)
+        return self.hf[-1][:, 0]
+
+    def backward(self, dyhat):
+        """dyhat: [B] FP32 loss gradient of the predictions.  Returns the
+        gradients (weights, biases), FP32."""
+        torch = self.torch
+        B = dyhat.shape[0]
+        if dyhat.dim() != 1 or B != self.hb[0].shape[0] or dyhat.dtype != torch.float32:
+            raise ValueError("Mlp.backward: gradient must be FP32 [B] for the last forward batch")
+        L = len(self.W)
+        dz = dyhat.reshape(B, 1).contiguous()
+        dzb = torch.empty((B, 1), dtype=torch.bfloat16, device=self.device)
+        native._check(_lib().ps_to_bf16(B, _ptr(dz), _ptr(dzb), self._stream()))
+        gW, gb = [None] * L, [None] * L
+        for l in range(L - 1, -1, -1):
+            n, k = self.W[l].shape
+            gW[l] = torch.empty((n, k), dtype=torch.float32, device=self.device)
+            gb[l] = torch.empty(n, dtype=torch.float32, device=self.device)
+            native._check(_lib().ps_gemm_bf16(n, k, B, _ptr(dzb), 1, n, _ptr(self.hb[l]), k, 1, _ptr(gW[l]), k, 0,
+                                              None, 0, None, 0, self._stream()))
+            native._check(_lib().ps_column_sum(B, n, _ptr(dz), _ptr(gb[l]), self._stream()))
+            if l > 0:
+                dh = torch.empty((B, k), dtype=torch.float32, device=self.device)
+                native._check(_lib().ps_gemm_bf16(B, k, n, _ptr(dzb), n, 1, _ptr(self.Wb[l]), k, 1, _ptr(dh), k, 0,
+                                                  None, 0, None, 0, self._stream()))
+                dz = torch.empty((B, k), dtype=torch.float32, device=self.device)
+                dzb = torch.empty((B, k), dtype=torch.bfloat16, device=self.device)
+                native._check(_lib().ps_relu_backward(B * k, _ptr(dh), _ptr(self.hf[l]), _ptr(dz), _ptr(dzb),
+                                                      self._stream()))
+        return gW, gb
+
+    def adam(self, gW, gb, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
+        self.steps += 1
+        for l in range(len(self.W)):
+            native._check(_lib().ps_adam_step(self.W[l].numel(), _ptr(self.W[l]), _ptr(gW[l]), _ptr(self.mW[l]),
+                                              _ptr(self.vW[l]), lr, beta1, beta2, eps, self.steps,
+                                              _ptr(self.Wb[l]), self._stream()))
+            native._check(_lib().ps_adam_step(self.b[l].numel(), _ptr(self.b[l]), _ptr(gb[l]), _ptr(self.mb[l]),
+                                              _ptr(self.vb[l]), lr, beta1, beta2, eps, self.steps, None,
+                                              self._stream()))
+
+    def train_step(self, xb, y, lr=1e-3):
+        """One Adam step on the mean squared error; returns the loss."""
+        yhat = self.forward(xb)
+        diff = yhat - y
+        loss = float((diff * diff).mean())
+        gW, gb = self.backward((2.0 / len(y)) * diff)
+        self.adam(gW, gb, lr)
+        return loss
+
+    def predict(self, feat):
+        torch = self.torch
+        x = torch.from_numpy(np.ascontiguousarray(feat, dtype=np.float32)).to(self.device).to(torch.bfloat16)
+        out = []
+        for i in range(0, x.shape[0], 8192):
+            out.append(self.forward(x[i:i + 8192]).cpu().numpy())
+        return np.concatenate(out)
+
+    def state(self):
+        d = {"sizes": np.array(self.sizes)}
+        for l in range(len(self.W)):
+            d[f"W{l}"] = self.W[l].cpu().numpy()
+            d[f"b{l}"] = self.b[l].cpu().numpy()
+        return d
+
+    @classmethod
+    def from_state(cls, d, device="cuda"):
+        net = cls(tuple(int(v) for v in d["sizes"]), device=device)
+        for l in range(len(net.W)):
+            net.W[l].copy_(net.torch.from_numpy(np.asarray(d[f"W{l}"], dtype=np.float32)))
+            net.b[l].copy_(net.torch.from_numpy(np.asarray(d[f"b{l}"], dtype=np.float32)))
+        net._sync_bf16()
+        return net
+
+
+def select(pred, top=0.034, halo=1, audit=0.02, seed=0):
+    """Frequency indices (0-based) to fit: the `top` share with the lowest
+    predicted rms, each with `halo` neighbours on either side (an LM minimum
+    in frequency is a few grid steps wide, finer than the folded features
+    resolve), plus an `audit` share drawn uniformly from the rest.  The
+    defaults fit at most 12.2 % of the grid."""
+    n = len(pred)
+    k = max(1, int(round(top * n)))
+    order = np.argsort(pred, kind="stable")
+    chosen = set()
+    for i in order[:k].tolist():
+        for d in range(-halo, halo + 1):
+            if 0 <= i + d < n:
+                chosen.add(i + d)
+    rest = np.array(sorted(set(range(n)) - chosen), dtype=np.int64)
+    na = min(len(rest), max(1, int(round(audit * n))))
+    rng = np.random.default_rng(seed)
+    if na:
+        chosen.update(rng.choice(rest, size=na, replace=False).tolist())
+    return np.array(sorted(chosen), dtype=np.int64)
+
+
+def screened_scan(obj, net, conw_r, top=0.034, halo=1, audit=0.02, seed=0, device=0,
+                  precision=native.PRECISION_FP64):
+    """Fits only the screened frequencies (after the convexity-weight search,
+    whose conw_r is passed in).  Returns (frequency indices 1-based, lines,
+    per-fit results)."""
+    pred = net.predict(normalise(features(obj, frequencies(obj), device)))
+    idx = select(pred, top, halo, audit, seed) + 1
+    nf = np.repeat(idx, native.N_POLES).astype(np.int32)
+    pl = np.tile(np.arange(native.N_POLES), len(idx)).astype(np.int32)
+    with native.Engine(obj, device) as eng:
+        eng.set_precision(precision)
+        eng.configure(conw_r=conw_r)
+        res, niter, status = eng.fit_items(nf, pl)
+    res = res.reshape(len(idx), native.N_POLES, 6)
+    lines = np.zeros((len(idx), 6))
+    for q in range(len(idx)):
+        r = res[q]
+        best = -1
+        for p in range(native.N_POLES):   # NaN-safe, earliest pole wins ties
+            if best < 0 or (not np.isnan(r[p, 0]) and not (r[p, 0] >= r[best, 0])):
+                best = p
+        b = r[best]
+        lines[q] = (24 * b[2], b[0], b[0] * b[0] * obj.n_points, b[1], b[3], b[4])
+    return idx, lines, res
+
+
+def best_line(lines):
+    """Index of the lowest-rms line (NaN lines never win)."""
+    r = np.where(np.isnan(lines[:, 1]), np.inf, lines[:, 1])
+    return int(np.argmin(r))
+
+
+def load_model(path=MODEL_PATH, device="cuda"):
+    """The trained screening network (written by screen_train)."""
+    return Mlp.from_state(np.load(path), device=device)

@@ -1,0 +1,57 @@
+"""CPU checks of the screening restatement (oracle/screen_ref.py) that the
+GPU tests compare the kernels with: BF16 rounding, the fold statistics on a
+known periodic signal, and the network's backward pass against finite
+differences."""
+import numpy as np
+
+from oracle import screen_ref
+
+
+def test_bf16_round():
+    x = np.array([1.0, 1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -8, -2.5, 3.0e38, 0.0], dtype=np.float32)
+    r = screen_ref.bf16_round(x)
+    assert list(r[:4]) == [1.0, 1.0, 1.0 + 2 * 2.0 ** -7, -2.5]   # ties go to the even neighbour
+    assert r[5] == 0.0
+    u = r.view(np.uint32)
+    assert np.all(u & 0xFFFF == 0)
+
+
+def test_fold_statistics_of_a_double_peaked_curve():
+    rng = np.random.default_rng(0)
+    f0 = 3.7                                            # rotations per day
+    t = np.sort(rng.uniform(0.0, 40.0, 600))
+    br = 1.0 + 0.2 * np.cos(2 * np.pi * 2 * f0 * t + 0.3) + 0.002 * rng.standard_normal(600)
+    lens = [300, 300]
+    at = screen_ref.features(t, br, lens, [f0, 1.2345])
+    # at the rotation frequency: little dispersion, power in the second harmonic
+    theta64_all = at[0, 64 + 0]
+    h2_all = at[0, 64 + 5]
+    assert theta64_all < 0.05 and h2_all > 0.9
+    # at an unrelated frequency the fold explains little
+    assert at[1, 64 + 3] > 0.5 and at[1, 64 + 0] > 10 * theta64_all
+    assert at.shape == (2, 88)
+
+
+def test_network_backward_matches_finite_differences():
+    rng = np.random.default_rng(1)
+    sizes = (6, 5, 4, 1)
+    W = [rng.standard_normal((n, k)) * 0.7 for k, n in zip(sizes[:-1], sizes[1:])]
+    b = [rng.standard_normal(n) * 0.1 for n in sizes[1:]]
+    x = rng.standard_normal((9, 6))
+    y = rng.standard_normal(9)
+    loss, _, gW, gb = screen_ref.mlp_forward_backward(x, y, W, b, round_bf16=False)
+    h = 1e-6
+    for l in range(len(W)):
+        for (i, j) in [(0, 0), (W[l].shape[0] - 1, W[l].shape[1] - 1)]:
+            Wp = [w.copy() for w in W]
+            Wp[l][i, j] += h
+            lp = screen_ref.mlp_forward_backward(x, y, Wp, b, round_bf16=False)[0]
+            Wp[l][i, j] -= 2 * h
+            lm = screen_ref.mlp_forward_backward(x, y, Wp, b, round_bf16=False)[0]
+            assert abs((lp - lm) / (2 * h) - gW[l][i, j]) < 1e-6 * max(1.0, abs(gW[l][i, j]))
+        bp = [v.copy() for v in b]
+        bp[l][0] += h
+        lp = screen_ref.mlp_forward_backward(x, y, W, bp, round_bf16=False)[0]
+        bp[l][0] -= 2 * h
+        lm = screen_ref.mlp_forward_backward(x, y, W, bp, round_bf16=False)[0]
+        assert abs((lp - lm) / (2 * h) - gb[l][0]) < 1e-6 * max(1.0, abs(gb[l][0]))
