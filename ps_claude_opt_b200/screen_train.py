@@ -178,27 +178,33 @@ def main():
     ap.add_argument("--epochs", type=int, default=150)
     ap.add_argument("--labels", default=None, help="npz of training labels: read if present, else written")
     ap.add_argument("--fulls", default=None, help="npz of held-out full scans: read if present, else written")
+    ap.add_argument("--eval-start", type=int, default=0, help="first held-out object (seed offset)")
+    ap.add_argument("--model", default=None, help="judge this trained network instead of training one")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
     t0 = time.time()
-    if args.labels and os.path.exists(args.labels):
-        labels = load_labels(args.labels)
+    if args.model:
+        net = screen.load_model(args.model)
     else:
-        labels = label_objects(args.objects)
-        if args.labels:
-            save_labels(args.labels, labels)
-    X, Y = training_set(labels)
-    print("training set: %d samples from %d objects, %.1f s" % (len(Y), len(labels), time.time() - t0), flush=True)
-    net = train(X, Y, args.epochs)
-    if args.out:
-        np.savez_compressed(args.out, **net.state())
+        if args.labels and os.path.exists(args.labels):
+            labels = load_labels(args.labels)
+        else:
+            labels = label_objects(args.objects)
+            if args.labels:
+                save_labels(args.labels, labels)
+        X, Y = training_set(labels)
+        print("training set: %d samples from %d objects, %.1f s" % (len(Y), len(labels), time.time() - t0),
+              flush=True)
+        net = train(X, Y, args.epochs)
+        if args.out:
+            np.savez_compressed(args.out, **net.state())
     if args.eval_objects:
         if args.fulls and os.path.exists(args.fulls):
             d = np.load(args.fulls)
             fulls = [(int(s), d[f"lines{i}"], float(d["conw"][i]), float(d["secs"][i]))
                      for i, s in enumerate(d["seeds"])]
         else:
-            fulls = full_scans(args.eval_objects)
+            fulls = full_scans(args.eval_objects, seed0=EVAL_SEED + args.eval_start)
             if args.fulls:
                 np.savez_compressed(args.fulls, seeds=np.array([f[0] for f in fulls]),
                                     conw=np.array([f[2] for f in fulls]), secs=np.array([f[3] for f in fulls]),
