@@ -362,7 +362,11 @@ def main():
                              (ctas * nsm * (obj.n_points * (obj.ma + 2) + obj.n_curves * (obj.ma + 3)) * 8 / 1e6),
                        "parallelism": "dp%d (disjoint frequency ranges per GPU)" % world},
             "s_per_object": n_obj / (value / world),
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "roofline": {"bound": "tensor",
+                         "bound_detail": "FP64 compute: the FP64 tensor-core (DMMA) and FMA pipes share one "
+                                         "capacity on B200 (probe: 37.0 / 34.9 TF/s alone, 36.5 together); "
+                                         "MEASURED_PEAKS.json's bf16 figure does not apply to FP64 work",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": NCU_DRAM_BYTES_PER_FIT * n_fits,
                          "traffic_source": "ncu capture of the profile case (148 fits), scaled by fits per launch",
                          "peak_source": "measured FP64 FMA probe (ps_measure_fp64_peak) on this GPU; "
