@@ -381,7 +381,7 @@ def main():
                                "vs_plain_fp64_full_scan_s": n_obj / (value / world),
                                "note": "top 3.4 % of the network's ranking with one neighbour each side plus a "
                                        "2 % random audit; mixed-precision fits; trained network from "
-                                       "ps_claude_opt_b200/screen_model.npz"},
+                                       "ps_claude_opt_b200/screen_model.bin"},
             "mixed": {"value": mixed_value, "unit": "fits/s", "ms_per_step": mixed_ms / args.steps,
                       "s_per_object": n_obj / (mixed_value / world), "gpu_launches": args.steps,
                       "precision": "facet sweep FP32 with 3xTF32 tensor-core shape derivatives; geometry, "

@@ -260,6 +260,17 @@ ps_status ps_screen_features(int32_t device, int32_t n_points, const double *tim
                              const double *brightness, const ps_curves *curves, int32_t n_freq,
                              const double *freqs, float *features);
 
+/* Scores of n_freq trial frequencies (1/hour) from a trained screening
+   network: lower = more promising.  The 88 features above, standardised per
+   feature over these frequencies, pass through n_layers dense layers
+   (sizes[0] = 88 .. sizes[n_layers] = 1, ReLU between them, BF16 operands,
+   FP32 accumulation); params holds each layer's weights [out][in] then its
+   biases [out], FP32, layer after layer. */
+ps_status ps_screen_rank(int32_t device, int32_t n_points, const double *tim,
+                         const double *brightness, const ps_curves *curves, int32_t n_freq,
+                         const double *freqs_per_hour, int32_t n_layers, const int32_t *sizes,
+                         const float *params, float *score);
+
 /* Device-pointer kernels of the screening network (BF16 operands, FP32
    accumulation on the tensor cores).  ps_gemm_bf16: C[m][n] (+)= sum_k
    A[m*sam + k*sak] B[k*sbk + n*sbn] (+ bias[n]) (ReLU if relu), written to

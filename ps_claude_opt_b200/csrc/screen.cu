@@ -22,6 +22,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -426,5 +427,84 @@ extern "C" ps_status ps_to_bf16(int64_t n, const float *x, void *y, void *stream
     if (n == 0) return PS_OK;
     to_bf16_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, x, (__nv_bfloat16 *)y);
     SC_CUDA(cudaGetLastError());
+    return PS_OK;
+}
+
+extern "C" ps_status ps_screen_rank(int32_t device, int32_t n_points, const double *tim, const double *brightness,
+                                    const ps_curves *curves, int32_t n_freq, const double *freqs_per_hour,
+                                    int32_t n_layers, const int32_t *sizes, const float *params, float *score)
+{
+    if (n_freq < 0 || (n_freq > 0 && (!freqs_per_hour || !score)) || n_layers < 1 || n_layers > 16 || !sizes ||
+        !params)
+        return psb_fail(PS_ERR_ARG, "ps_screen_rank: bad arguments");
+    if (sizes[0] != kFeatures || sizes[n_layers] != 1)
+        return psb_fail(PS_ERR_ARG, "ps_screen_rank: the network must map 88 features to 1 score");
+    for (int l = 1; l < n_layers; ++l)
+        if (sizes[l] < 1 || sizes[l] > 4096) return psb_fail(PS_ERR_ARG, "ps_screen_rank: layer width 1..4096");
+    if (n_freq == 0) return PS_OK;
+    // features (1/day), then standardised per feature over this object's frequencies
+    std::vector<double> fday(n_freq);
+    for (int f = 0; f < n_freq; ++f) fday[f] = 24.0 * freqs_per_hour[f];
+    std::vector<float> feat((size_t)n_freq * kFeatures);
+    ps_status st = ps_screen_features(device, n_points, tim, brightness, curves, n_freq, fday.data(), feat.data());
+    if (st != PS_OK) return st;
+    for (int k = 0; k < kFeatures; ++k) {
+        double m = 0, m2 = 0;
+        for (int f = 0; f < n_freq; ++f) m += feat[(size_t)f * kFeatures + k];
+        m /= n_freq;
+        for (int f = 0; f < n_freq; ++f) {
+            const double d = feat[(size_t)f * kFeatures + k] - m;
+            m2 += d * d;
+        }
+        const double sd = std::sqrt(m2 / n_freq);
+        const double inv = sd > 1e-6 ? 1.0 / sd : 1.0;
+        for (int f = 0; f < n_freq; ++f) {
+            float &v = feat[(size_t)f * kFeatures + k];
+            v = (float)((v - m) * inv);
+        }
+    }
+    // device buffers: parameters (FP32 + BF16 copies), two activation buffers
+    size_t n_par = 0, widest = kFeatures;
+    for (int l = 0; l < n_layers; ++l) {
+        n_par += (size_t)sizes[l + 1] * sizes[l] + sizes[l + 1];
+        widest = std::max<size_t>(widest, (size_t)sizes[l + 1]);
+    }
+    float *d_par = nullptr, *d_out = nullptr;
+    __nv_bfloat16 *d_parb = nullptr, *d_h[2] = {nullptr, nullptr};
+    cudaError_t e = cudaMalloc(&d_par, sizeof(float) * n_par);
+    if (e == cudaSuccess) e = cudaMalloc(&d_parb, sizeof(__nv_bfloat16) * n_par);
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(float) * ((size_t)n_freq * widest + n_freq * kFeatures));
+    if (e == cudaSuccess) e = cudaMalloc(&d_h[0], sizeof(__nv_bfloat16) * (size_t)n_freq * widest);
+    if (e == cudaSuccess) e = cudaMalloc(&d_h[1], sizeof(__nv_bfloat16) * (size_t)n_freq * widest);
+    float *d_feat = d_out + (size_t)n_freq * widest;
+    if (e == cudaSuccess) e = cudaMemcpy(d_par, params, sizeof(float) * n_par, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d_feat, feat.data(), sizeof(float) * feat.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        to_bf16_kernel<<<blocks_for((long)n_par, 256), 256>>>((long)n_par, d_par, d_parb);
+        to_bf16_kernel<<<blocks_for((long)feat.size(), 256), 256>>>((long)feat.size(), d_feat, d_h[0]);
+        e = cudaGetLastError();
+    }
+    size_t off = 0;
+    int cur = 0;
+    for (int l = 0; l < n_layers && e == cudaSuccess; ++l) {
+        const int k = sizes[l], n = sizes[l + 1];
+        const __nv_bfloat16 *W = d_parb + off;
+        const float *b = d_par + off + (size_t)n * k;
+        off += (size_t)n * k + n;
+        const bool last = l == n_layers - 1;
+        dim3 grid((n + kGemmTN - 1) / kGemmTN, (n_freq + kGemmTM - 1) / kGemmTM);
+        gemm_bf16_kernel<<<grid, 128>>>(n_freq, n, k, d_h[cur], k, 1, W, 1, k, last ? d_out : nullptr, n, 0, b,
+                                        last ? 0 : 1, last ? nullptr : d_h[1 - cur], n);
+        e = cudaGetLastError();
+        cur = 1 - cur;
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(score, d_out, sizeof(float) * n_freq, cudaMemcpyDeviceToHost);
+    cudaFree(d_par);
+    cudaFree(d_parb);
+    cudaFree(d_out);
+    cudaFree(d_h[0]);
+    cudaFree(d_h[1]);
+    if (e != cudaSuccess) return psb_fail_cuda(e, "ps_screen_rank");
     return PS_OK;
 }

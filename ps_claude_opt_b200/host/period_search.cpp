@@ -25,6 +25,12 @@
 //     --fresh        ignore an existing state file
 //     --stop-after N exit after N chunks, as an interrupted run would
 //     --dump-object  print the prepared object (hex floats) and exit, no GPU
+//     --precision P  fp64 (default) or mixed (FP32 facet sweep, 3xTF32
+//                    tensor-core shape derivatives, FP64 elsewhere)
+//     --screen MODEL fit only the frequencies a trained screening network
+//                    ranks first (the top 3.4 % with one neighbour on either
+//                    side, plus a 2 % audit sample); one output line per
+//                    fitted frequency, in frequency order; no checkpoints
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -43,15 +49,17 @@ namespace {
 struct Options {
     int device = 0;
     std::string in = "period_search_in", out = "period_search_out", state = "period_search_state";
-    int chunk = 1024, max_freq = 0, quirks = 0, stop_after = 0;
+    int chunk = 1024, max_freq = 0, quirks = 0, stop_after = 0, precision = PS_PRECISION_FP64;
     bool fresh = false, dump = false;
+    std::string screen;
 };
 
 int usage()
 {
     std::fprintf(stderr,
                  "usage: period_search [-d device] [-s state] [--chunk N] [--max-freq N] [--quirks Q] [--fresh]\n"
-                 "                     [--stop-after N] [--dump-object] [input [output]]\n");
+                 "                     [--stop-after N] [--dump-object] [--precision fp64|mixed] [--screen MODEL]\n"
+                 "                     [input [output]]\n");
     return 2;
 }
 
@@ -82,6 +90,15 @@ bool parse_args(int argc, char **argv, Options &o)
             o.fresh = true;
         } else if (a == "--dump-object") {
             o.dump = true;
+        } else if (a == "--precision") {
+            if (i + 1 >= argc) return false;
+            const std::string v = argv[++i];
+            if (v == "fp64") o.precision = PS_PRECISION_FP64;
+            else if (v == "mixed") o.precision = PS_PRECISION_MIXED;
+            else return false;
+        } else if (a == "--screen") {
+            if (i + 1 >= argc) return false;
+            o.screen = argv[++i];
         } else if (!a.empty() && a[0] == '-') {
             return false;
         } else if (pos == 0) {
@@ -145,6 +162,64 @@ std::FILE *reopen_output(const std::string &path, int nlines)
     return f;
 }
 
+// A screening network file: "PSMLP001", int32 layer count, int32 sizes,
+// then float32 weights [out][in] and biases [out] per layer.
+bool read_model(const std::string &path, std::vector<int32_t> &sizes, std::vector<float> &params)
+{
+    std::FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return false;
+    char magic[8];
+    int32_t nl = 0;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PSMLP001", 8) == 0 &&
+              std::fread(&nl, 4, 1, f) == 1 && nl >= 1 && nl <= 16;
+    if (ok) {
+        sizes.resize(nl + 1);
+        ok = std::fread(sizes.data(), 4, nl + 1, f) == (size_t)(nl + 1);
+    }
+    size_t n = 0;
+    if (ok)
+        for (int l = 0; l < nl; ++l) n += (size_t)sizes[l + 1] * sizes[l] + sizes[l + 1];
+    if (ok) {
+        params.resize(n);
+        ok = std::fread(params.data(), 4, n, f) == n && std::fgetc(f) == EOF;
+    }
+    std::fclose(f);
+    return ok;
+}
+
+// The frequencies (0-based) a screened scan fits: the lowest-scoring
+// `top` share with `halo` neighbours each side, plus an `audit` share of the
+// rest drawn by a partial Fisher-Yates shuffle from a 64-bit linear
+// congruential generator (the Python screen draws the same sample).
+std::vector<int> screen_select(const std::vector<float> &score, double top, int halo, double audit, uint64_t seed)
+{
+    const int n = (int)score.size();
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return score[a] < score[b]; });
+    const int k = std::max(1, (int)std::nearbyint(top * n));
+    std::vector<char> chosen(n, 0);
+    for (int r = 0; r < k; ++r)
+        for (int d = -halo; d <= halo; ++d)
+            if (order[r] + d >= 0 && order[r] + d < n) chosen[order[r] + d] = 1;
+    std::vector<int> rest;
+    for (int i = 0; i < n; ++i)
+        if (!chosen[i]) rest.push_back(i);
+    const int na = std::min((int)rest.size(), std::max(1, (int)std::nearbyint(audit * n)));
+    uint64_t x = seed * 2654435761ull + 1ull;
+    for (int j = 0; j < na; ++j) {
+        x = 6364136223846793005ull * x + 1442695040888963407ull;
+        const uint64_t r = x >> 33;
+        const int pick = j + (int)(r % (uint64_t)(rest.size() - j));
+        std::swap(rest[j], rest[pick]);
+        chosen[rest[j]] = 1;
+    }
+    std::vector<int> out;
+    for (int i = 0; i < n; ++i)
+        if (chosen[i]) out.push_back(i);
+    return out;
+}
+
 int fail(const char *what)
 {
     std::fprintf(stderr, "period_search: %s: %s\n", what, ps_last_error());
@@ -190,6 +265,10 @@ int main(int argc, char **argv)
                        obj.weight.data(), &h) != PS_OK)
         return fail("prepare");
     if (opt.quirks) ps_gpu_set_quirks(h, opt.quirks);
+    if (ps_gpu_set_precision(h, opt.precision) != PS_OK) {
+        ps_gpu_unprepare(h);
+        return fail("precision");
+    }
 
     const ps_curves curves{obj.n_curves, obj.curve_len.data(), obj.curve_rel.data()};
     const ps_shape shape{obj.n_coef, obj.normal.data(), obj.d_area.data(), obj.d_sphere.data()};
@@ -226,6 +305,58 @@ int main(int argc, char **argv)
 
     int n_last = obj.n_max;
     if (opt.max_freq > 0 && opt.max_freq < n_last) n_last = opt.max_freq;
+
+    if (!opt.screen.empty()) {
+        // screened scan: rank every frequency, fit the chosen ones
+        std::vector<int32_t> sizes;
+        std::vector<float> params;
+        if (!read_model(opt.screen, sizes, params)) {
+            std::fprintf(stderr, "period_search: cannot read screening model %s\n", opt.screen.c_str());
+            std::fclose(out);
+            ps_gpu_unprepare(h);
+            return 1;
+        }
+        std::vector<double> freqs(n_last);
+        for (int f = 0; f < n_last; ++f) freqs[f] = obj.freq_start - f * obj.freq_step;
+        std::vector<float> score(n_last);
+        if (ps_screen_rank(opt.device, obj.n_points, obj.tim.data(), obj.brightness.data(), &curves, n_last,
+                           freqs.data(), (int32_t)sizes.size() - 1, sizes.data(), params.data(),
+                           score.data()) != PS_OK) {
+            std::fclose(out);
+            ps_gpu_unprepare(h);
+            return fail("screen");
+        }
+        const std::vector<int> sel = screen_select(score, 0.034, 1, 0.02, 0);
+        std::vector<int32_t> nf, pl;
+        for (int f : sel)
+            for (int p = 0; p < PS_N_POLES; ++p) {
+                nf.push_back(f + 1);
+                pl.push_back(p);
+            }
+        std::vector<ps_fit_result> res(nf.size());
+        if (ps_gpu_configure(h, obj.freq_start, obj.freq_step, obj.stop_condition, obj.n_iter_min, conw_r, conw_r,
+                             obj.n_points, obj.ia.data(), ia_par, obj.cg_first.data(), obj.sig.data(),
+                             obj.sigr2.data(), obj.n_fac, obj.brightness.data(), &curves, &shape) != PS_OK ||
+            ps_gpu_fit_items(h, (int32_t)nf.size(), nf.data(), pl.data(), res.data()) != PS_OK) {
+            std::fclose(out);
+            ps_gpu_unprepare(h);
+            return fail("screened scan");
+        }
+        for (size_t q = 0; q < sel.size(); ++q) {
+            const ps_fit_result *r = &res[q * PS_N_POLES];
+            int best = -1;  // NaN-safe, earliest pole wins ties (start_CUDA.cu:1200-1229)
+            for (int p = 0; p < PS_N_POLES; ++p)
+                if (best < 0 || (!std::isnan(r[p].dev) && !(r[p].dev >= r[best].dev))) best = p;
+            const ps_fit_result &b = r[best];
+            const ps_line l{24 * b.per, b.dev, b.dev * b.dev * obj.n_points,
+                            sel[q] == 0 ? conw_r * obj.escl * obj.escl : b.dark, b.lambda_deg, b.beta_deg};
+            print_line(out, l);
+        }
+        std::fclose(out);
+        std::fprintf(stderr, "period_search: screened scan fitted %zu of %d frequencies\n", sel.size(), n_last);
+        ps_gpu_unprepare(h);
+        return 0;
+    }
     std::vector<ps_line> lines(opt.chunk);
     int chunks = 0;
     for (int n = nlines + 1; n <= n_last;) {

@@ -95,6 +95,8 @@ _SIGS = {
     "ps_gpu_set_precision": (C.c_int, [C.c_void_p, C.c_int32]),
     "ps_screen_features": (C.c_int, [C.c_int32, C.c_int32, _dp, _dp, C.POINTER(Curves), C.c_int32, _dp,
                                      C.POINTER(C.c_float)]),
+    "ps_screen_rank": (C.c_int, [C.c_int32, C.c_int32, _dp, _dp, C.POINTER(Curves), C.c_int32, _dp, C.c_int32,
+                                 _ip, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "ps_gemm_bf16": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
                                C.c_int64, C.c_int64, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32,
                                C.c_void_p, C.c_int32, C.c_void_p]),

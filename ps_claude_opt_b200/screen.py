@@ -19,7 +19,8 @@ from . import native
 
 import os
 
-MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "screen_model.npz")
+MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "screen_model.bin")
+MODEL_MAGIC = b"PSMLP001"
 N_FEATURES = 88
 SIZES = (N_FEATURES, 256, 256, 256, 1)   # features -> 3 x 256 hidden -> predicted log rms
 
@@ -54,10 +55,12 @@ def features(obj, freqs, device=0):
 
 def normalise(feat):
     """Per-object standardisation of each feature over the object's
-    frequencies: the network ranks frequencies within one object."""
-    mu = feat.mean(0)
-    sd = feat.std(0)
-    return ((feat - mu) / np.where(sd > 1e-6, sd, 1.0)).astype(np.float32)
+    frequencies (in float64, as ps_screen_rank does): the network ranks
+    frequencies within one object."""
+    f = np.asarray(feat, dtype=np.float64)
+    mu = f.mean(0)
+    sd = np.sqrt(((f - mu) ** 2).mean(0))
+    return ((f - mu) / np.where(sd > 1e-6, sd, 1.0)).astype(np.float32)
 
 
 def _ptr(t):
@@ -188,6 +191,18 @@ class Mlp:
         return net
 
 
+def _lcg_uniform(seed, n):
+    """n uniform integers in [0, 2^31) from the 64-bit linear congruential
+    generator x <- 6364136223846793005 x + 1442695040888963407 (the host
+    program draws the same audit sample)."""
+    x = (int(seed) * 2654435761 + 1) & 0xFFFFFFFFFFFFFFFF
+    out = []
+    for _ in range(n):
+        x = (6364136223846793005 * x + 1442695040888963407) & 0xFFFFFFFFFFFFFFFF
+        out.append(x >> 33)
+    return out
+
+
 def select(pred, top=0.034, halo=1, audit=0.02, seed=0):
     """Frequency indices (0-based) to fit: the `top` share with the lowest
     predicted rms, each with `halo` neighbours on either side (an LM minimum
@@ -196,17 +211,19 @@ def select(pred, top=0.034, halo=1, audit=0.02, seed=0):
     defaults fit at most 12.2 % of the grid."""
     n = len(pred)
     k = max(1, int(round(top * n)))
-    order = np.argsort(pred, kind="stable")
+    order = np.argsort(np.asarray(pred), kind="stable")
     chosen = set()
     for i in order[:k].tolist():
         for d in range(-halo, halo + 1):
             if 0 <= i + d < n:
                 chosen.add(i + d)
-    rest = np.array(sorted(set(range(n)) - chosen), dtype=np.int64)
+    rest = [i for i in range(n) if i not in chosen]
     na = min(len(rest), max(1, int(round(audit * n))))
-    rng = np.random.default_rng(seed)
-    if na:
-        chosen.update(rng.choice(rest, size=na, replace=False).tolist())
+    # partial Fisher-Yates shuffle of the rest, driven by the LCG
+    for j, r in enumerate(_lcg_uniform(seed, na)):
+        pick = j + r % (len(rest) - j)
+        rest[j], rest[pick] = rest[pick], rest[j]
+    chosen.update(rest[:na])
     return np.array(sorted(chosen), dtype=np.int64)
 
 
@@ -242,6 +259,58 @@ def best_line(lines):
     return int(np.argmin(r))
 
 
+def save_model(path, state):
+    """Writes a network state as MODEL_MAGIC, int32 layer count, int32 sizes,
+    then per layer float32 weights [out][in] and biases [out]
+    (little-endian) -- the layout ps_screen_rank takes."""
+    sizes = [int(v) for v in state["sizes"]]
+    with open(path, "wb") as f:
+        f.write(MODEL_MAGIC)
+        np.array([len(sizes) - 1] + sizes, dtype="<i4").tofile(f)
+        for l in range(len(sizes) - 1):
+            np.asarray(state[f"W{l}"], dtype="<f4").tofile(f)
+            np.asarray(state[f"b{l}"], dtype="<f4").tofile(f)
+
+
+def read_model(path=MODEL_PATH):
+    """(sizes, flat float32 parameters, state dict) of a model file."""
+    with open(path, "rb") as f:
+        if f.read(8) != MODEL_MAGIC:
+            raise ValueError("not a screening model file: " + path)
+        nl = int(np.fromfile(f, dtype="<i4", count=1)[0])
+        sizes = np.fromfile(f, dtype="<i4", count=nl + 1)
+        params = np.fromfile(f, dtype="<f4")
+    state, off = {"sizes": sizes}, 0
+    for l in range(nl):
+        n, k = int(sizes[l + 1]), int(sizes[l])
+        state[f"W{l}"] = params[off:off + n * k].reshape(n, k)
+        off += n * k
+        state[f"b{l}"] = params[off:off + n]
+        off += n
+    if off != len(params):
+        raise ValueError("screening model file size does not match its layer sizes: " + path)
+    return sizes, params, state
+
+
 def load_model(path=MODEL_PATH, device="cuda"):
     """The trained screening network (written by screen_train)."""
-    return Mlp.from_state(np.load(path), device=device)
+    return Mlp.from_state(read_model(path)[2], device=device)
+
+
+def rank(obj, path=MODEL_PATH, device=0):
+    """Scores of all grid frequencies through the C ABI (ps_screen_rank)."""
+    sizes, params, _ = read_model(path)
+    freqs = np.ascontiguousarray(frequencies(obj), dtype=np.float64)
+    score = np.zeros(len(freqs), dtype=np.float32)
+    tim = np.ascontiguousarray(obj.tim, dtype=np.float64)
+    br = np.ascontiguousarray(obj.brightness, dtype=np.float64)
+    cl = np.ascontiguousarray(obj.curve_len, dtype=np.int32)
+    cr = np.ascontiguousarray(obj.curve_rel, dtype=np.int32)
+    curves = native.Curves(len(cl), cl.ctypes.data_as(C.POINTER(C.c_int32)), cr.ctypes.data_as(C.POINTER(C.c_int32)))
+    sz = np.ascontiguousarray(sizes, dtype=np.int32)
+    native._check(native.lib().ps_screen_rank(device, len(tim), native._p(tim), native._p(br), C.byref(curves),
+                                              len(freqs), native._p(freqs), len(sz) - 1,
+                                              sz.ctypes.data_as(C.POINTER(C.c_int32)),
+                                              params.ctypes.data_as(C.POINTER(C.c_float)),
+                                              score.ctypes.data_as(C.POINTER(C.c_float))))
+    return score

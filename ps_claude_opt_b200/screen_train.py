@@ -1,6 +1,6 @@
 """Trains the frequency-screening network and judges it against the full scan.
 
-    python -m ps_claude_opt_b200.screen_train --objects 96 --out ps_claude_opt_b200/screen_model.npz
+    python -m ps_claude_opt_b200.screen_train --objects 96 --out ps_claude_opt_b200/screen_model.bin
 
 Training objects come from the production-size generator (lmax 6, 512 facets,
 40 dense relative curves + 400 calibrated points, periods 2-100 h on the
@@ -197,7 +197,7 @@ def main():
               flush=True)
         net = train(X, Y, args.epochs)
         if args.out:
-            np.savez_compressed(args.out, **net.state())
+            screen.save_model(args.out, net.state())
     if args.eval_objects:
         if args.fulls and os.path.exists(args.fulls):
             d = np.load(args.fulls)

@@ -55,3 +55,36 @@ def test_network_backward_matches_finite_differences():
         bp[l][0] -= 2 * h
         lm = screen_ref.mlp_forward_backward(x, y, W, bp, round_bf16=False)[0]
         assert abs((lp - lm) / (2 * h) - gb[l][0]) < 1e-6 * max(1.0, abs(gb[l][0]))
+
+
+def test_model_file_round_trip_and_errors(tmp_path):
+    from ps_claude_opt_b200 import screen
+
+    rng = np.random.default_rng(2)
+    state = {"sizes": np.array([88, 7, 1])}
+    state["W0"], state["b0"] = rng.standard_normal((7, 88)).astype(np.float32), rng.standard_normal(7).astype(np.float32)
+    state["W1"], state["b1"] = rng.standard_normal((1, 7)).astype(np.float32), rng.standard_normal(1).astype(np.float32)
+    p = tmp_path / "m.bin"
+    screen.save_model(str(p), state)
+    sizes, params, back = screen.read_model(str(p))
+    assert list(sizes) == [88, 7, 1] and params.size == 88 * 7 + 7 + 7 + 1
+    for k in ("W0", "b0", "W1", "b1"):
+        assert np.array_equal(back[k], state[k])
+    p.write_bytes(p.read_bytes()[:-4])                     # truncated
+    import pytest
+    with pytest.raises(ValueError):
+        screen.read_model(str(p))
+    sizes, _, _ = screen.read_model()                       # the committed model
+    assert list(sizes) == [88, 256, 256, 256, 1]
+
+
+def test_selection_is_deterministic_and_bounded():
+    from ps_claude_opt_b200 import screen
+
+    pred = np.random.default_rng(5).standard_normal(5000)
+    a, b = screen.select(pred), screen.select(pred)
+    assert np.array_equal(a, b)
+    assert len(a) <= 0.122 * 5000 + 1
+    top = np.argsort(pred, kind="stable")[:170]
+    assert set(top.tolist()) <= set(a.tolist())
+    assert np.all(np.diff(a) > 0)

@@ -46,3 +46,63 @@ def test_screened_scan_in_mixed_precision_finds_the_same_line():
     b = screen.best_line(lines)
     assert idx[b] == row["best_freq"]
     assert abs(lines[b, 0] - row["best_line"][0]) < 1e-4 and abs(lines[b, 1] - row["best_line"][1]) < 1e-4
+
+
+def test_rank_through_the_c_abi_matches_the_python_network():
+    from ps_claude_opt_b200 import screen, screen_train
+
+    row = json.load(open(FIXTURE))[1]
+    obj, _ = screen_train.make_object(row["seed"])
+    got = screen.rank(obj)
+    ref = screen.load_model().predict(screen.normalise(screen.features(obj, screen.frequencies(obj))))
+    assert np.max(np.abs(got - ref)) < 1e-3
+    assert np.array_equal(screen.select(got), screen.select(ref))
+
+
+def _write_input(tmp_path, seed):
+    from ps_claude_opt_b200 import synth
+
+    cfg = synth.SynthConfig(l_max=6, m_max=6, nrows=8, n_dense=40, dense_pts=(50, 120), n_sparse=400,
+                            sparse_curves=2, period_range=(2.0, 100.0), n_freq=5000)
+    text, _ = synth.generate(cfg, seed)
+    (tmp_path / "period_search_in").write_text(text)
+
+
+def _lines(path):
+    return np.array([[float(v) for v in l.split()] for l in path.read_text().splitlines()])
+
+
+def test_host_program_screened_scan_finds_the_best_line(tmp_path):
+    import subprocess
+
+    from ps_claude_opt_b200 import native, screen
+
+    row = json.load(open(FIXTURE))[0]
+    _write_input(tmp_path, row["seed"])
+    r = subprocess.run([native.HOST_PROGRAM, "--screen", screen.MODEL_PATH], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    lines = _lines(tmp_path / "period_search_out")
+    assert len(lines) <= 0.125 * row["n_freq"]
+    b = int(np.argmin(lines[:, 1]))
+    assert abs(lines[b, 0] - row["best_line"][0]) < 1e-6           # period [h], as printed
+    assert abs(lines[b, 1] - row["best_line"][1]) < 1e-6           # rms
+    assert abs(lines[b, 4] - round(row["best_line"][4])) <= 1 and abs(lines[b, 5] - round(row["best_line"][5])) <= 1
+
+
+def test_host_program_mixed_precision_scan(tmp_path):
+    import subprocess
+
+    from conftest import synth_text
+    from ps_claude_opt_b200 import native
+
+    text, _ = synth_text("c1", 11)
+    (tmp_path / "period_search_in").write_text(text)
+    for prec, name in (("fp64", "out64"), ("mixed", "outmx")):
+        r = subprocess.run([native.HOST_PROGRAM, "--precision", prec, "--fresh", "-s", "st_" + prec,
+                            "period_search_in", name], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+    a, b = _lines(tmp_path / "out64"), _lines(tmp_path / "outmx")
+    assert a.shape == b.shape
+    assert np.all(np.abs(a[:, 0] - b[:, 0]) < 0.1) and np.all(np.abs(a[:, 1] - b[:, 1]) < 0.1)
+    assert int(np.argmin(a[:, 1])) == int(np.argmin(b[:, 1]))
