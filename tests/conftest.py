@@ -37,6 +37,14 @@ def synth_text(kind: str, seed: int):
                                    sparse_curves=1, n_freq=3),
         # lmax 8, relative data only (87 fitted parameters)
         "lmax8rel": synth.SynthConfig(l_max=8, m_max=8, nrows=10, n_dense=5, dense_pts=(30, 40), n_freq=3),
+        # calibrated data only: no relative curve, no renormalisation
+        "calonly": synth.SynthConfig(l_max=4, m_max=4, nrows=6, n_dense=0, n_sparse=150, sparse_curves=3, n_freq=3),
+        # ragged: relative curves of 1 to 3 points beside one calibrated curve
+        "ragged": synth.SynthConfig(l_max=3, m_max=3, nrows=5, n_dense=12, dense_pts=(1, 3), n_sparse=40,
+                                    sparse_curves=1, n_freq=3),
+        # the largest input: 199 lightcurves (200 with the pseudo-curve, the
+        # reference's MAX_LC) of 100 points = 19 900 points, lmax 8, 800 facets
+        "maxsize": synth.SynthConfig(l_max=8, m_max=8, nrows=10, n_dense=199, dense_pts=(100, 100), n_freq=2),
     }
     text, truth = synth.generate(cfgs[kind], seed)
     return text, truth

@@ -40,7 +40,8 @@ def _with_weights(text):
     return text.rstrip("\n") + "\n1 0.5\n3 2.5\n"
 
 
-@pytest.mark.parametrize("kind,weights", [("tiny", False), ("mixed", False), ("mixed", True), ("c2", False)])
+@pytest.mark.parametrize("kind,weights", [("tiny", False), ("mixed", False), ("mixed", True), ("c2", False),
+                                          ("calonly", False), ("ragged", False)])
 def test_reader_matches_python(kind, weights, tmp_path):
     from ps_claude_opt_b200 import objects
 

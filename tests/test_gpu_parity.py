@@ -25,7 +25,7 @@ def _close(g, o, rel):
     return np.abs(g - o).max() <= rel * scale
 
 
-@pytest.mark.parametrize("kind", ["tiny", "c1", "mixed", "c2", "lmax8", "lmax8rel"])
+@pytest.mark.parametrize("kind", ["tiny", "c1", "mixed", "c2", "lmax8", "lmax8rel", "calonly", "ragged", "maxsize"])
 def test_eval_matches_oracle(kind):
     import oracle
     from ps_claude_opt_b200 import native, objects
@@ -64,7 +64,7 @@ def _fit_both(kind, n_iter, nfreq=3):
     return g, gi, gs, o, oi, os_
 
 
-@pytest.mark.parametrize("kind", ["tiny", "c1", "mixed", "lmax8"])
+@pytest.mark.parametrize("kind", ["tiny", "c1", "mixed", "lmax8", "calonly", "ragged"])
 def test_short_fits_match_oracle(kind):
     """Three LM iterations: the damped solve, accept/reject, lambda update, rms
     and the per-fit result agree tightly before round-off can steer the two
