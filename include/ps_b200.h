@@ -148,11 +148,14 @@ typedef struct ps_object {
 
 /* The reference's whole flow -- convexity-weight search (CUDAPrecalc), then
    the scan (CUDAStart) -- for n_obj objects at once (no counterpart in the
-   reference, which runs one object per process).  Each search round and the
-   scans of all objects are enqueued on a few streams, so the GPU stays full
-   while small objects' launches start and end.  Lines of object i go to
-   lines[line_offset[i] .. + n_lines[i]); the final convexity weight to
-   conw_r_out[i].  quirks: PS_QUIRK_* for every object. */
+   reference, which runs one object per process).  Objects of one padded
+   coefficient count share one persistent FP64 launch whose device queue
+   holds all their (frequency, pole) items, so uneven objects and ragged
+   iteration counts even out over the CTAs; each search round is one launch
+   per group, and the scans of all groups are one captured CUDA graph.
+   Lines of object i go to lines[line_offset[i] .. + n_lines[i]); the final
+   convexity weight to conw_r_out[i].  quirks: PS_QUIRK_* for every
+   object. */
 ps_status ps_gpu_scan_batch(int32_t device, int32_t n_obj, const ps_object *objs, int32_t quirks,
                             ps_line *lines, const int64_t *line_offset, int32_t *n_lines,
                             double *conw_r_out);

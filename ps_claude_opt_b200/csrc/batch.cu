@@ -4,19 +4,21 @@
 // The reference runs one object per process (period_search_BOINC.cpp:
 // 638-872): a convexity-weight search of 100 fits per round
 // (start_CUDA.cu:400-789) -- too few to fill 148 SMs -- and then the scan.
-// Here every object gets its own handle (tables, items, results), and the
-// launches of all objects go to kSlots streams: each search round launches
-// every still-searching object at once, and the scans follow, so kernels of
-// different objects overlap and the tail of one object's persistent launch
-// is filled by the next object's CTAs.  Objects go to slots largest first,
-// each to the slot with the least work so far.  A slot's launches run one
-// after another and share its scratch and queue counter; every launch
-// zeroes the counter on the slot's stream before it starts.
+// Here the objects are grouped by padded coefficient count (one kernel
+// instance each) and every group runs as ONE persistent launch whose device
+// queue holds the (frequency, pole) items of all its objects: an item's pole
+// field carries its object, and a CTA reloads the object's facet table when
+// its next item belongs to another object (items are ordered by object, so
+// that is rare).  Ragged iteration counts and uneven object sizes even out
+// across the CTAs.  Each search round launches every group once with the
+// items of the objects still searching; the scan launches of all groups are
+// captured into one CUDA graph (a fork over the groups' streams and a join)
+// and replayed.  The groups' launches run concurrently on their streams.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
-#include <numeric>
+#include <map>
 #include <vector>
 
 #include "engine.h"
@@ -26,27 +28,45 @@
 
 namespace {
 
-constexpr int kSlots = 4;
 constexpr int kTestPeriods = 10;  // start_CUDA.cu:420
 
-struct Slot {
+struct Group {
+    int ncp = 0;
+    std::vector<int> members;          // object indices
+    psb::DevObject env{};              // largest sizes: the shared-memory layout
+    size_t per_cta = 0;                // scratch doubles of one CTA (largest object)
+    int ctas = 0;                      // resident CTAs of the batch kernel
     cudaStream_t stream = nullptr;
+    cudaEvent_t join = nullptr;
+    psb::DevBuf<psb::DevObject> objs;
+    psb::DevBuf<psb::DevParams> prms;
+    psb::DevBuf<psb::FitItem> items;
+    psb::DevBuf<psb::FitOut> out;
     psb::DevBuf<double> scratch;
-    psb::DevBuf<int> queue;
-    size_t scratch_doubles = 0;
+    psb::DevBuf<int> queue, status;
 };
 
 struct Batch {
     std::vector<ps_gpu *> h;
-    Slot slot[kSlots];
+    std::vector<Group> groups;
+    cudaStream_t origin = nullptr;
+    cudaEvent_t fork = nullptr;
     ~Batch()
     {
-        for (Slot &s : slot) {
-            if (s.stream) cudaStreamSynchronize(s.stream);
-            s.scratch.release();
-            s.queue.release();
-            if (s.stream) cudaStreamDestroy(s.stream);
+        for (Group &g : groups) {
+            if (g.stream) cudaStreamSynchronize(g.stream);
+            g.objs.release();
+            g.prms.release();
+            g.items.release();
+            g.out.release();
+            g.scratch.release();
+            g.queue.release();
+            g.status.release();
+            if (g.join) cudaEventDestroy(g.join);
+            if (g.stream) cudaStreamDestroy(g.stream);
         }
+        if (fork) cudaEventDestroy(fork);
+        if (origin) cudaStreamDestroy(origin);
         for (ps_gpu *x : h) ps_gpu_unprepare(x);
     }
 };
@@ -58,49 +78,161 @@ ps_status configure(ps_gpu *h, const ps_object &o, double conw_r, double conw_r_
                             &o.shape);
 }
 
-// Uploads the items of each job, launches all jobs on their slots and
-// brings the results back.  job = (object index, items).
-ps_status run_jobs(Batch &b, const std::vector<int> &slot_of, const std::vector<std::pair<int, std::vector<psb::FitItem>>> &jobs,
-                   std::vector<std::vector<psb::FitOut>> &res)
-{
-    res.assign(jobs.size(), {});
-    // everything a launch reads is on the device before the first launch
-    for (Slot &s : b.slot) {
-        if (s.scratch_doubles) PSB_CUDA(s.scratch.ensure(s.scratch_doubles));
-        PSB_CUDA(s.queue.ensure(1));
-    }
-    for (const auto &j : jobs) {
-        ps_gpu *h = b.h[j.first];
-        PSB_CUDA(psb::upload(h->items, j.second, h->stream));
-        PSB_CUDA(h->out.ensure(j.second.size()));
-        PSB_CUDA(cudaStreamSynchronize(h->stream));
-    }
-    for (const auto &j : jobs) {
-        ps_gpu *h = b.h[j.first];
-        Slot &s = b.slot[slot_of[j.first]];
-        const int n = (int)j.second.size();
-        if (n == 0) continue;
-        const int n_ctas = std::max(1, std::min(n, h->ctas_per_sm * h->n_sm));
-        PSB_CUDA(cudaMemsetAsync(s.queue.ptr, 0, sizeof(int), s.stream));
-        const int e = psb::launch_fits(h->obj, h->prm, h->items.ptr, n, s.queue.ptr, h->out.ptr, s.scratch.ptr,
-                                       h->scratch_per_cta, n_ctas, h->status.ptr, s.stream);
-        if (e) return psb_fail_cuda(e, "ps_gpu_scan_batch: fit kernel launch");
-    }
-    for (Slot &s : b.slot) PSB_CUDA(cudaStreamSynchronize(s.stream));
-    for (size_t k = 0; k < jobs.size(); ++k) {
-        ps_gpu *h = b.h[jobs[k].first];
-        res[k].resize(jobs[k].second.size());
-        if (!res[k].empty())
-            PSB_CUDA(cudaMemcpy(res[k].data(), h->out.ptr, res[k].size() * sizeof(psb::FitOut),
-                                cudaMemcpyDeviceToHost));
-    }
-    return PS_OK;
-}
-
 int scan_lines(const ps_object &o)
 {
     const int n_max = (int)((o.freq_start - o.freq_end) / o.freq_step) + 1;
     return std::max(0, std::min(n_max - o.n_start_from + 1, (int)o.max_lines));
+}
+
+// Shared-memory layout of a group: the largest sizes of its objects, the
+// preferred tile layout that fits (beside the kernel's static object copy).
+ps_status plan_group(Batch &b, Group &g, size_t smem_limit)
+{
+    psb::DevObject &e = g.env;
+    e = b.h[g.members[0]]->obj;
+    for (int i : g.members) {
+        const psb::DevObject &o = b.h[i]->obj;
+        e.n_fac = std::max(e.n_fac, o.n_fac);
+        e.mfit = std::max(e.mfit, o.mfit);
+        e.n_curves = std::max(e.n_curves, o.n_curves);
+        e.row_stride = std::max(e.row_stride, o.row_stride);
+        e.ma = std::max(e.ma, o.ma);
+    }
+    const int layouts[3][2] = {{32, 1}, {32, 0}, {16, 0}};
+    bool ok = false;
+    for (const auto &l : layouts) {
+        e.tile_rows = l[0];
+        e.cstat_smem = l[1];
+        if (psb::fit_smem_bytes(e.n_fac, e.mfit, e.ncp, e.n_curves, e.row_stride, e.tile_rows, e.cstat_smem, 0) +
+                1024 <= smem_limit) {
+            ok = true;
+            break;
+        }
+    }
+    if (!ok) return psb_fail(PS_ERR_ARG, "ps_gpu_scan_batch: objects too large for shared memory");
+    g.per_cta = 0;
+    for (int i : g.members) {
+        psb::DevObject o = b.h[i]->obj;
+        o.tile_rows = e.tile_rows;
+        o.cstat_smem = e.cstat_smem;
+        g.per_cta = std::max(g.per_cta, psb::fit_scratch_doubles(o));
+    }
+    const int per_sm = psb::fit_batch_ctas_per_sm(e);
+    if (per_sm < 1) return psb_fail(PS_ERR_CUDA, "ps_gpu_scan_batch: batch kernel cannot be resident");
+    g.ctas = per_sm * b.h[g.members[0]]->n_sm;
+    return PS_OK;
+}
+
+// The group's objects (their current constants) to the device.
+ps_status upload_objects(Batch &b, Group &g)
+{
+    std::vector<psb::DevObject> objs;
+    std::vector<psb::DevParams> prms;
+    for (int i : g.members) {
+        psb::DevObject o = b.h[i]->obj;
+        o.tile_rows = g.env.tile_rows;
+        o.cstat_smem = g.env.cstat_smem;
+        objs.push_back(o);
+        psb::DevParams p = b.h[i]->prm;
+        p.phase_cycles = nullptr;
+        prms.push_back(p);
+    }
+    PSB_CUDA(psb::upload(g.objs, objs, g.stream));
+    PSB_CUDA(psb::upload(g.prms, prms, g.stream));
+    return PS_OK;
+}
+
+// Items of one launch per group: for member k of group g, items[k] (n_freq,
+// pole) pairs.  Uploads, launches (captured into a graph when `graph`), and
+// returns each member's results.
+ps_status run_groups(Batch &b, const std::vector<std::vector<std::vector<psb::FitItem>>> &items, bool graph,
+                     std::vector<std::vector<std::vector<psb::FitOut>>> &res)
+{
+    res.assign(b.groups.size(), {});
+    std::vector<std::vector<int>> offset(b.groups.size());
+    std::vector<int> total(b.groups.size(), 0);
+    for (size_t gi = 0; gi < b.groups.size(); ++gi) {
+        Group &g = b.groups[gi];
+        std::vector<psb::FitItem> flat;
+        for (size_t k = 0; k < g.members.size(); ++k) {
+            offset[gi].push_back((int)flat.size());
+            for (psb::FitItem it : items[gi][k]) {
+                it.pole |= (int)k << 8;
+                flat.push_back(it);
+            }
+        }
+        total[gi] = (int)flat.size();
+        if (flat.empty()) continue;
+        PSB_CUDA(psb::upload(g.items, flat, g.stream));
+        PSB_CUDA(g.out.ensure(flat.size()));
+        PSB_CUDA(g.scratch.ensure(g.per_cta * (size_t)std::min(g.ctas, total[gi])));
+        PSB_CUDA(g.queue.ensure(1));
+        if (!g.status.ptr) {
+            PSB_CUDA(g.status.ensure(1));
+            PSB_CUDA(cudaMemsetAsync(g.status.ptr, 0, sizeof(int), g.stream));
+        }
+        PSB_CUDA(cudaStreamSynchronize(g.stream));  // uploads done before any capture
+        const int e = psb::prepare_batch_kernel(g.env);
+        if (e) return psb_fail_cuda(e, "ps_gpu_scan_batch: kernel attributes");
+    }
+    auto enqueue = [&](size_t gi) -> ps_status {
+        Group &g = b.groups[gi];
+        PSB_CUDA(cudaMemsetAsync(g.queue.ptr, 0, sizeof(int), g.stream));
+        const int e = psb::launch_fits_batch(g.env, g.objs.ptr, g.prms.ptr, g.items.ptr, total[gi], g.queue.ptr,
+                                             g.out.ptr, g.scratch.ptr, g.per_cta, std::min(g.ctas, total[gi]),
+                                             g.status.ptr, g.stream);
+        if (e) return psb_fail_cuda(e, "ps_gpu_scan_batch: fit kernel launch");
+        return PS_OK;
+    };
+    if (graph) {
+        cudaGraph_t gr = nullptr;
+        cudaGraphExec_t ex = nullptr;
+        PSB_CUDA(cudaStreamBeginCapture(b.origin, cudaStreamCaptureModeThreadLocal));
+        ps_status st = PS_OK;
+        cudaError_t ce = cudaEventRecord(b.fork, b.origin);
+        for (size_t gi = 0; gi < b.groups.size() && st == PS_OK && ce == cudaSuccess; ++gi) {
+            if (!total[gi]) continue;
+            Group &g = b.groups[gi];
+            ce = cudaStreamWaitEvent(g.stream, b.fork, 0);
+            if (ce == cudaSuccess) st = enqueue(gi);
+            if (st == PS_OK && ce == cudaSuccess) ce = cudaEventRecord(g.join, g.stream);
+            if (st == PS_OK && ce == cudaSuccess) ce = cudaStreamWaitEvent(b.origin, g.join, 0);
+        }
+        const cudaError_t ee = cudaStreamEndCapture(b.origin, &gr);
+        if (st != PS_OK) {
+            if (gr) cudaGraphDestroy(gr);
+            return st;
+        }
+        if (ce != cudaSuccess || ee != cudaSuccess) {
+            if (gr) cudaGraphDestroy(gr);
+            return psb_fail_cuda(ce != cudaSuccess ? ce : ee, "ps_gpu_scan_batch: graph capture");
+        }
+        ce = cudaGraphInstantiate(&ex, gr, 0);
+        if (ce == cudaSuccess) ce = cudaGraphLaunch(ex, b.origin);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(b.origin);
+        if (ex) cudaGraphExecDestroy(ex);
+        cudaGraphDestroy(gr);
+        if (ce != cudaSuccess) return psb_fail_cuda(ce, "ps_gpu_scan_batch: graph launch");
+    } else {
+        for (size_t gi = 0; gi < b.groups.size(); ++gi) {
+            if (!total[gi]) continue;
+            ps_status st = enqueue(gi);
+            if (st != PS_OK) return st;
+        }
+        for (Group &g : b.groups) PSB_CUDA(cudaStreamSynchronize(g.stream));
+    }
+    for (size_t gi = 0; gi < b.groups.size(); ++gi) {
+        Group &g = b.groups[gi];
+        std::vector<psb::FitOut> all(total[gi]);
+        if (total[gi])
+            PSB_CUDA(cudaMemcpy(all.data(), g.out.ptr, sizeof(psb::FitOut) * total[gi], cudaMemcpyDeviceToHost));
+        res[gi].resize(g.members.size());
+        for (size_t k = 0; k < g.members.size(); ++k) {
+            const int n = (int)items[gi][k].size();
+            res[gi][k].assign(all.begin() + offset[gi][k], all.begin() + offset[gi][k] + n);
+        }
+    }
+    return PS_OK;
 }
 
 }  // namespace
@@ -127,30 +259,30 @@ extern "C" ps_status ps_gpu_scan_batch(int32_t device, int32_t n_obj, const ps_o
                                       o.alamda_incrr, o.ee, o.ee0, o.tim, o.phi0, o.ndata, o.weight, &b.h[i]);
         if (st != PS_OK) return st;
         b.h[i]->quirks = quirks;
-        // a first configure validates the object and sizes its scratch
+        // a first configure validates the object and builds its device tables
         st = configure(b.h[i], o, o.conw_r, o.conw_r);
         if (st != PS_OK) return st;
     }
     PSB_CUDA(cudaSetDevice(device));
-    for (Slot &s : b.slot) PSB_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
-
-    // slots: largest object first, each to the least-loaded slot
-    std::vector<double> cost(n_obj);
+    cudaDeviceProp prop;
+    PSB_CUDA(cudaGetDeviceProperties(&prop, device));
+    PSB_CUDA(cudaStreamCreateWithFlags(&b.origin, cudaStreamNonBlocking));
+    PSB_CUDA(cudaEventCreateWithFlags(&b.fork, cudaEventDisableTiming));
+    std::map<int, int> by_ncp;
     for (int i = 0; i < n_obj; ++i) {
-        const psb::DevObject &d = b.h[i]->obj;
-        cost[i] = (double)(scan_lines(objs[i]) + kTestPeriods) * d.n_points * d.n_fac * d.ncp;
+        const int ncp = b.h[i]->obj.ncp;
+        if (!by_ncp.count(ncp)) {
+            by_ncp[ncp] = (int)b.groups.size();
+            b.groups.emplace_back();
+            b.groups.back().ncp = ncp;
+        }
+        b.groups[by_ncp[ncp]].members.push_back(i);
     }
-    std::vector<int> order(n_obj), slot_of(n_obj);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
-    double load[kSlots] = {0, 0, 0, 0};
-    for (int i : order) {
-        const int s = (int)(std::min_element(load, load + kSlots) - load);
-        slot_of[i] = s;
-        load[s] += cost[i];
-        ps_gpu *h = b.h[i];
-        const int n_ctas = h->ctas_per_sm * h->n_sm;
-        b.slot[s].scratch_doubles = std::max(b.slot[s].scratch_doubles, h->scratch_per_cta * (size_t)n_ctas);
+    for (Group &g : b.groups) {
+        PSB_CUDA(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+        PSB_CUDA(cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming));
+        ps_status st = plan_group(b, g, prop.sharedMemPerBlockOptin);
+        if (st != PS_OK) return st;
     }
 
     // convexity-weight search, all objects' rounds together
@@ -162,61 +294,81 @@ extern "C" ps_status ps_gpu_scan_batch(int32_t device, int32_t n_obj, const ps_o
     for (int n = 1; n <= kTestPeriods; ++n)
         for (int pl = 0; pl < PS_N_POLES; ++pl) test_items.push_back(psb::FitItem{n, pl});
     for (;;) {
-        std::vector<std::pair<int, std::vector<psb::FitItem>>> jobs;
-        for (int i = 0; i < n_obj; ++i) {
-            if (new_conw[i] == 1 || !(conw[i] * objs[i].escl * objs[i].escl < 10.0)) continue;
-            const double rms_w = (quirks & PS_QUIRK_PRECALC_CONW) ? 0.0 : conw[i];
-            ps_status st = configure(b.h[i], objs[i], conw[i], rms_w);
+        bool any = false;
+        std::vector<std::vector<std::vector<psb::FitItem>>> items(b.groups.size());
+        for (size_t gi = 0; gi < b.groups.size(); ++gi) {
+            Group &g = b.groups[gi];
+            items[gi].resize(g.members.size());
+            for (size_t k = 0; k < g.members.size(); ++k) {
+                const int i = g.members[k];
+                if (new_conw[i] == 1 || !(conw[i] * objs[i].escl * objs[i].escl < 10.0)) continue;
+                const double rms_w = (quirks & PS_QUIRK_PRECALC_CONW) ? 0.0 : conw[i];
+                ps_status st = configure(b.h[i], objs[i], conw[i], rms_w);
+                if (st != PS_OK) return st;
+                items[gi][k] = test_items;
+                any = true;
+            }
+            ps_status st = upload_objects(b, g);
             if (st != PS_OK) return st;
-            jobs.emplace_back(i, test_items);
         }
-        if (jobs.empty()) break;
-        std::vector<std::vector<psb::FitOut>> res;
-        ps_status st = run_jobs(b, slot_of, jobs, res);
+        if (!any) break;
+        std::vector<std::vector<std::vector<psb::FitOut>>> res;
+        ps_status st = run_groups(b, items, false, res);
         if (st != PS_OK) return st;
-        for (size_t k = 0; k < jobs.size(); ++k) {
-            const int i = jobs[k].first;
-            double sum_dark = 0.0;
-            for (int t = 0; t < kTestPeriods; ++t)
-                sum_dark = sum_dark + res[k][t * PS_N_POLES + psb_best_pole(&res[k][t * PS_N_POLES])].dark;
-            const double ave = sum_dark / kTestPeriods;
-            if (ave < 1.0) new_conw[i] = 1;
-            if (ave >= 1.0) conw[i] = conw[i] * 2;
-        }
+        for (size_t gi = 0; gi < b.groups.size(); ++gi)
+            for (size_t k = 0; k < b.groups[gi].members.size(); ++k) {
+                if (items[gi][k].empty()) continue;
+                const int i = b.groups[gi].members[k];
+                const std::vector<psb::FitOut> &r = res[gi][k];
+                double sum_dark = 0.0;
+                for (int t = 0; t < kTestPeriods; ++t)
+                    sum_dark = sum_dark + r[t * PS_N_POLES + psb_best_pole(&r[t * PS_N_POLES])].dark;
+                const double ave = sum_dark / kTestPeriods;
+                if (ave < 1.0) new_conw[i] = 1;
+                if (ave >= 1.0) conw[i] = conw[i] * 2;
+            }
     }
 
-    // the scans (start_CUDA.cu:792-1245)
-    std::vector<std::pair<int, std::vector<psb::FitItem>>> jobs;
-    for (int i = 0; i < n_obj; ++i) {
-        conw_r_out[i] = conw[i];
-        ps_status st = configure(b.h[i], objs[i], conw[i], conw[i]);
-        if (st != PS_OK) return st;
-        std::vector<psb::FitItem> items;
-        const int nl = scan_lines(objs[i]);
-        items.reserve((size_t)nl * PS_N_POLES);
-        for (int q = 0; q < nl; ++q)
-            for (int pl = 0; pl < PS_N_POLES; ++pl) items.push_back(psb::FitItem{objs[i].n_start_from + q, pl});
-        jobs.emplace_back(i, std::move(items));
-    }
-    std::vector<std::vector<psb::FitOut>> res;
-    ps_status st = run_jobs(b, slot_of, jobs, res);
-    if (st != PS_OK) return st;
-    for (int i = 0; i < n_obj; ++i) {
-        const ps_object &o = objs[i];
-        const int nl = scan_lines(o);
-        ps_line *out = lines + line_offset[i];
-        for (int q = 0; q < nl; ++q) {
-            const psb::FitOut *r = &res[i][(size_t)q * PS_N_POLES];
-            const psb::FitOut &bp = r[psb_best_pole(r)];
-            ps_line &L = out[q];
-            L.period_h = 24 * bp.per;
-            L.rms = bp.dev;
-            L.chisq = bp.dev * bp.dev * o.ndata;
-            L.dark = (o.n_start_from + q == 1) ? conw[i] * o.escl * o.escl : bp.dark;
-            L.lambda_deg = bp.lambda_deg;
-            L.beta_deg = bp.beta_deg;
+    // the scans (start_CUDA.cu:792-1245), one graph over all groups
+    std::vector<std::vector<std::vector<psb::FitItem>>> items(b.groups.size());
+    for (size_t gi = 0; gi < b.groups.size(); ++gi) {
+        Group &g = b.groups[gi];
+        items[gi].resize(g.members.size());
+        for (size_t k = 0; k < g.members.size(); ++k) {
+            const int i = g.members[k];
+            conw_r_out[i] = conw[i];
+            ps_status st = configure(b.h[i], objs[i], conw[i], conw[i]);
+            if (st != PS_OK) return st;
+            const int nl = scan_lines(objs[i]);
+            items[gi][k].reserve((size_t)nl * PS_N_POLES);
+            for (int q = 0; q < nl; ++q)
+                for (int pl = 0; pl < PS_N_POLES; ++pl)
+                    items[gi][k].push_back(psb::FitItem{objs[i].n_start_from + q, pl});
         }
-        n_lines[i] = nl;
+        ps_status st = upload_objects(b, g);
+        if (st != PS_OK) return st;
     }
+    std::vector<std::vector<std::vector<psb::FitOut>>> res;
+    ps_status st = run_groups(b, items, true, res);
+    if (st != PS_OK) return st;
+    for (size_t gi = 0; gi < b.groups.size(); ++gi)
+        for (size_t k = 0; k < b.groups[gi].members.size(); ++k) {
+            const int i = b.groups[gi].members[k];
+            const ps_object &o = objs[i];
+            const int nl = scan_lines(o);
+            ps_line *out = lines + line_offset[i];
+            for (int q = 0; q < nl; ++q) {
+                const psb::FitOut *r = &res[gi][k][(size_t)q * PS_N_POLES];
+                const psb::FitOut &bp = r[psb_best_pole(r)];
+                ps_line &L = out[q];
+                L.period_h = 24 * bp.per;
+                L.rms = bp.dev;
+                L.chisq = bp.dev * bp.dev * o.ndata;
+                L.dark = (o.n_start_from + q == 1) ? conw[i] * o.escl * o.escl : bp.dark;
+                L.lambda_deg = bp.lambda_deg;
+                L.beta_deg = bp.beta_deg;
+            }
+            n_lines[i] = nl;
+        }
     return PS_OK;
 }

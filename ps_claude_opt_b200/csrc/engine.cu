@@ -7,7 +7,7 @@
 namespace psb {
 
 using KernelFn = void (*)(DevObject, DevParams, const FitItem *, int, int *, FitOut *, double *, size_t,
-                          int *, EvalOut, int);
+                          int *, EvalOut, int, const DevObject *, const DevParams *);
 
 // The shape-derivative accumulators live in registers, so the kernel is
 // compiled per padded coefficient count.
@@ -46,6 +46,22 @@ PSB_NCP_LIST(PSB_DECL)
 #define PSB_DECLM(N) KernelFn fit_kernel_mixed_ptr_##N();
 PSB_MIXED_LIST(PSB_DECLM)
 #undef PSB_DECLM
+#define PSB_DECLB(N) KernelFn fit_kernel_batch_ptr_##N();
+PSB_NCP_LIST(PSB_DECLB)
+#undef PSB_DECLB
+
+static KernelFn batch_kernel_for(int ncp)
+{
+    switch (ncp) {
+#define PSB_CASEB(N) \
+    case N:          \
+        return fit_kernel_batch_ptr_##N();
+        PSB_NCP_LIST(PSB_CASEB)
+#undef PSB_CASEB
+    default:
+        return nullptr;
+    }
+}
 
 static KernelFn kernel_for(int ncp, int mixed)
 {
@@ -99,7 +115,42 @@ int launch_fits(const DevObject &o, const DevParams &p, const FitItem *items, in
     if (e) return e;
     EvalOut ev{};
     fn<<<n_ctas, kThreads, smem, (cudaStream_t)stream>>>(o, p, items, n_items, queue, out, scratch,
-                                                         scratch_per_cta, status, ev, 0);
+                                                         scratch_per_cta, status, ev, 0, nullptr, nullptr);
+    return (int)cudaGetLastError();
+}
+
+int prepare_batch_kernel(const DevObject &env)
+{
+    KernelFn fn = batch_kernel_for(env.ncp);
+    if (!fn || env.mixed) return (int)cudaErrorInvalidValue;
+    const size_t smem = fit_smem_bytes(env.n_fac, env.mfit, env.ncp, env.n_curves, env.row_stride, env.tile_rows,
+                                       env.cstat_smem, 0);
+    return (int)cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+int fit_batch_ctas_per_sm(const DevObject &env)
+{
+    if (prepare_batch_kernel(env) != 0) return 0;
+    const size_t smem = fit_smem_bytes(env.n_fac, env.mfit, env.ncp, env.n_curves, env.row_stride, env.tile_rows,
+                                       env.cstat_smem, 0);
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel_for(env.ncp), kThreads, smem) != cudaSuccess)
+        return 0;
+    return n;
+}
+
+int launch_fits_batch(const DevObject &env, const DevObject *d_objs, const DevParams *d_prms, const FitItem *items,
+                      int n_items, int *queue, FitOut *out, double *scratch, size_t scratch_per_cta, int n_ctas,
+                      int *status, void *stream)
+{
+    KernelFn fn = batch_kernel_for(env.ncp);
+    if (!fn || env.mixed) return (int)cudaErrorInvalidValue;
+    const size_t smem = fit_smem_bytes(env.n_fac, env.mfit, env.ncp, env.n_curves, env.row_stride, env.tile_rows,
+                                       env.cstat_smem, 0);
+    DevParams p{};
+    EvalOut ev{};
+    fn<<<n_ctas, kThreads, smem, (cudaStream_t)stream>>>(env, p, items, n_items, queue, out, scratch,
+                                                         scratch_per_cta, status, ev, 0, d_objs, d_prms);
     return (int)cudaGetLastError();
 }
 
@@ -110,7 +161,7 @@ int launch_eval(const DevObject &o, const DevParams &p, EvalOut ev, double *scra
     int e = prepare_kernel(o, &fn, &smem);
     if (e) return e;
     fn<<<1, kThreads, smem, (cudaStream_t)stream>>>(o, p, nullptr, 1, nullptr, nullptr, scratch, 0, nullptr,
-                                                    ev, 1);
+                                                    ev, 1, nullptr, nullptr);
     return (int)cudaGetLastError();
 }
 

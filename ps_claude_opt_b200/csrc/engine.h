@@ -100,4 +100,17 @@ int launch_eval(const DevObject &o, const DevParams &p, EvalOut ev, double *scra
 // CTAs per SM the fit kernel reaches for this object.
 int fit_ctas_per_sm(const DevObject &o);
 
+// Many objects of one padded coefficient count in one persistent launch (FP64
+// kernel).  env carries the largest sizes of the objects (the shared-memory
+// layout: n_fac, mfit, n_curves, row_stride) and the common tile_rows and
+// cstat_smem; d_objs / d_prms are the objects' tables and constants on the
+// device, and an item's pole field is pole | object << 8.
+// prepare_batch_kernel sets the kernel's shared-memory limit (once, before
+// launching or capturing); launch_fits_batch only enqueues the launch.
+int prepare_batch_kernel(const DevObject &env);
+int fit_batch_ctas_per_sm(const DevObject &env);
+int launch_fits_batch(const DevObject &env, const DevObject *d_objs, const DevParams *d_prms, const FitItem *items,
+                      int n_items, int *queue, FitOut *out, double *scratch, size_t scratch_per_cta, int n_ctas,
+                      int *status, void *stream);
+
 }  // namespace psb

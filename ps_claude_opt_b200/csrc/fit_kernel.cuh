@@ -30,6 +30,8 @@ namespace psb {
 
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kTiny = 1e-8;
+constexpr int kPoleBits = 8;                  // FitItem::pole = pole | object << kPoleBits (batch)
+constexpr int kPoleMask = (1 << kPoleBits) - 1;
 constexpr int kStages = 4;          // basis chunks in flight in the facet sweep
 constexpr int kSortBands = 8;       // point sort: bands in cos(theta) ...
 constexpr int kSortSectors = 32;    // ... x sectors in longitude of the Sun-observer bisector
@@ -1530,23 +1532,178 @@ static __device__ int gauss_jordan(const Sh &s, int n)
 
 // ---------------------------------------------------------------- kernel
 
+// One (frequency, pole) fit, the whole LM loop, by the CTA; its result to
+// out[item].  o and p are the fit's object and constants.
 template <int NCP, bool MIXED>
+__device__ __forceinline__ void fit_one(const DevObject &o, const DevParams &p, const Sh &s, const FitItem it,
+                                        int item, FitOut *out, double *rows, int *status)
+{
+    const int tid = threadIdx.x;
+    const int nc = o.n_coef, ma = o.ma, mfit = o.mfit, ld = s.ld;
+    const int pole = it.pole & kPoleMask;
+    double *cstat = rows + (size_t)o.n_points * o.row_stride;
+    int *perm = reinterpret_cast<int *>(rows + scratch_perm(o.n_points, o.row_stride, o.n_curves, ma));
+
+    // initial parameters (CudaCalculatePreparePole, Start.cu:4346-4418)
+    if (tid == 0) {
+        double *a = s.a;
+        a[0] = 0;
+        for (int k = 1; k <= nc; ++k) a[k] = __ldg(&o.cg_first[k - 1]);
+        const double period = 1.0 / (p.freq_start - (it.n_freq - 1) * p.freq_step);
+        a[nc + 1] = (kPi / 180) * 90 - (kPi / 180) * p.beta_pole[pole];
+        a[nc + 2] = (kPi / 180) * p.lambda_pole[pole];
+        a[nc + 3] = (24.0 * 2.0 * kPi) / period;
+        a[nc + 4] = p.par[0];
+        a[nc + 5] = p.par[1];
+        a[nc + 6] = p.par[2];
+        a[ma - 1] = p.lcl;
+        a[ma] = 1;
+        s.scal[S_ALAMDA] = -1;
+        s.scal[S_ITERDIFF] = 1e40;
+        s.scal[S_DEVOLD] = 1e30;
+        s.scal[S_DEVNEW] = 0;
+        s.scal[S_CHCK] = 0;
+        s.ctl[C_NITER] = 0;
+        s.ctl[C_STATUS] = 0;
+    }
+    __syncthreads();
+
+    for (;;) {
+        // convergence test (CudaCalculateIter1Begin, Start.cu:4421-4462)
+        if (tid == 0) {
+            const int niter = s.ctl[C_NITER];
+            s.ctl[C_GO] = ((niter < p.n_iter_max) && (s.scal[S_ITERDIFF] > p.iter_diff_max)) ||
+                          (niter < p.n_iter_min);
+        }
+        __syncthreads();
+        if (!s.ctl[C_GO]) break;
+        const bool first = s.scal[S_ALAMDA] < 0;
+        __syncthreads();
+        if (first) {
+            if (tid == 0) s.scal[S_ALAMDA] = p.alamda_start;
+            double oc = evaluate<NCP, MIXED>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, perm, p.conw_r);
+            if (tid == 0) s.scal[S_OCHISQ] = oc;
+            for (int q = tid; q <= ma; q += kThreads) s.atry[q] = s.a[q];
+            __syncthreads();
+        }
+        // damped normal matrix and solve (mrqmin_1_end_opt)
+        const double ccc = 1 + s.scal[S_ALAMDA];
+        for (int idx = tid; idx < mfit * mfit; idx += kThreads) {
+            const int j = idx / mfit, k = idx - j * mfit;
+            const double v = s.alpha[j * ld + k];
+            s.covar[j * ld + k] = (j == k) ? v * ccc : v;
+        }
+        if (tid < mfit) s.da[tid] = s.beta[tid];
+        __syncthreads();
+        tmark(p, s, T_REST);
+        const int err = gauss_jordan(s, mfit);
+        tmark(p, s, T_SOLVE);
+        if (err == 0 || err == 2) {
+            if (tid < mfit) s.atry[s.fidx[tid]] = s.a[s.fidx[tid]] + s.da[tid];
+            if (err == 2 && tid == 0) s.ctl[C_STATUS] |= kStatusSingular;
+        }
+        __syncthreads();
+        const double chisq = evaluate<NCP, MIXED>(o, p, s, s.atry, s.covar, s.da, rows, cstat, perm, p.conw_r);
+        // accept / reject (mrqmin_2_end, Start.cu:300-392)
+        const bool accept = chisq < s.scal[S_OCHISQ];
+        __syncthreads();
+        if (accept) {
+            for (int idx = tid; idx < mfit * ld; idx += kThreads) s.alpha[idx] = s.covar[idx];
+            if (tid < mfit) s.beta[tid] = s.da[tid];
+            for (int q = tid; q <= ma; q += kThreads) s.a[q] = s.atry[q];
+        }
+        if (tid == 0) {
+            if (isnan(chisq)) s.ctl[C_STATUS] |= kStatusNanChisq;
+            if (accept) {
+                s.scal[S_ALAMDA] *= p.alamda_incrr;
+                s.scal[S_CHISQ] = chisq;
+            } else {
+                s.scal[S_ALAMDA] = p.alamda_incr * s.scal[S_ALAMDA];
+                s.scal[S_CHISQ] = s.scal[S_OCHISQ];
+            }
+            s.ctl[C_NITER] += 1;
+        }
+        __syncthreads();
+        // rms and convergence bookkeeping (CudaCalculateIter2, Start.cu:5129-5248)
+        const int niter = s.ctl[C_NITER];
+        const double ch = s.scal[S_CHISQ];
+        if (niter == 1 || ch < s.scal[S_OCHISQ]) {
+            __syncthreads();
+            const double area_sum = shape_areas(o, s, s.a);
+            double r[3] = {0, 0, 0};
+            for (int fi = tid; fi < o.n_fac; fi += kThreads) {
+                const double4 fr = s.F[fi];
+                r[0] += fr.w * fr.x;
+                r[1] += fr.w * fr.y;
+                r[2] += fr.w * fr.z;
+            }
+            block_sum<3>(r, s.red);
+            if (tid == 0) {
+                s.scal[S_OCHISQ] = ch;
+                s.scal[S_AREA] = area_sum;
+                const double aa = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+                const double rchisq = ch - aa * (p.conw_r_dev * p.conw_r_dev);
+                const double dev_new = sqrt(rchisq / (o.n_points + 3 - 3));
+                s.scal[S_DEVNEW] = dev_new;
+                s.scal[S_CHCK] = sqrt(aa);
+                const double diff = s.scal[S_DEVOLD] - dev_new;
+                if (diff > 1e-10) {
+                    s.scal[S_ITERDIFF] = diff;
+                    s.scal[S_DEVOLD] = dev_new;
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    // per-fit result (CudaCalculateFinishPole, Start.cu:5056-5125)
+    if (tid == 0) {
+        double dd = s.scal[S_CHCK] * 100.0 * (1.0 / s.scal[S_AREA]);
+        if (isnan(dd)) dd = 1.0;
+        const double la = (180 / kPi) * s.a[nc + 2];
+        FitOut r;
+        r.dev = s.scal[S_DEVNEW];
+        r.dark = dd;
+        r.per = 2 * kPi / s.a[nc + 3];
+        r.lambda_deg = la + (la < 0 ? 360 : 0);
+        r.beta_deg = 90 - (180 / kPi) * s.a[nc + 1];
+        r.chisq = s.scal[S_CHISQ];
+        r.niter = s.ctl[C_NITER];
+        r.status = s.ctl[C_STATUS] | (s.ctl[C_TIMEOUT] ? kStatusTimeout : 0);
+        out[item] = r;
+        if (r.status) atomicOr(status, r.status);
+        if (p.phase_cycles) {
+            tmark(p, s, T_REST);
+            for (int q = 0; q < T_NPHASE; ++q) {
+                atomicAdd(&p.phase_cycles[q], (unsigned long long)s.tclk[q]);
+                s.tclk[q] = 0;
+            }
+        }
+    }
+}
+
+template <int NCP, bool MIXED, bool BATCH>
 __global__ void __launch_bounds__(kThreads, 1)
 fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *queue, FitOut *out,
-           double *scratch, size_t scratch_per_cta, int *status, EvalOut ev, int mode)
+           double *scratch, size_t scratch_per_cta, int *status, EvalOut ev, int mode, const DevObject *objs,
+           const DevParams *prms)
 {
+    // batch launches: o holds the largest sizes of the batch (the shared-memory
+    // layout); every item names its object (FitItem::pole >> kPoleBits),
+    // whose tables and constants come from objs / prms when the CTA moves to it
+    __shared__ DevObject s_obj;
+    __shared__ DevParams s_prm;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Sh s;
     carve_bytes(o.n_fac, o.mfit, o.ncp, o.n_curves, o.row_stride, o.tile_rows, o.cstat_smem, MIXED ? 1 : 0, &s,
                 smem_raw);
     const int tid = threadIdx.x;
-    const int nc = o.n_coef, ma = o.ma, mfit = o.mfit, ld = s.ld;
     double *rows = scratch + (size_t)blockIdx.x * scratch_per_cta;
-    double *cstat = rows + (size_t)o.n_points * o.row_stride;
-    int *perm = reinterpret_cast<int *>(rows + scratch_perm(o.n_points, o.row_stride, o.n_curves, ma));
 
-    for (int f = tid; f < o.n_fac; f += kThreads) s.F[f] = ldg4(&o.facet[f]);
-    if (tid < mfit) s.fidx[tid] = __ldg(&o.fidx[tid]);
+    if constexpr (!BATCH) {
+        for (int f = tid; f < o.n_fac; f += kThreads) s.F[f] = ldg4(&o.facet[f]);
+        if (tid < o.mfit) s.fidx[tid] = __ldg(&o.fidx[tid]);
+    }
     if (tid == 0) {
         for (int b = 0; b < kStages; ++b) {
             mbar_init(&s.mbar[b], 1);
@@ -1564,164 +1721,50 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
     }
     __syncthreads();
 
-    if (mode == 1) {  // one stand-alone evaluation (parity hook)
-        for (int q = tid; q <= ma; q += kThreads) s.a[q] = ev.a[q];
-        __syncthreads();
-        double chisq = evaluate<NCP, MIXED>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, perm, p.conw_r);
-        for (int idx = tid; idx < mfit * mfit; idx += kThreads) {
-            const int j = idx / mfit, k = idx - j * mfit;
-            ev.alpha[idx] = s.alpha[j * ld + k];
+    if constexpr (!BATCH) {
+        if (mode == 1) {  // one stand-alone evaluation (parity hook)
+            const int ma = o.ma, mfit = o.mfit, ld = s.ld;
+            double *cstat = rows + (size_t)o.n_points * o.row_stride;
+            int *perm = reinterpret_cast<int *>(rows + scratch_perm(o.n_points, o.row_stride, o.n_curves, ma));
+            for (int q = tid; q <= ma; q += kThreads) s.a[q] = ev.a[q];
+            __syncthreads();
+            double chisq = evaluate<NCP, MIXED>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, perm, p.conw_r);
+            for (int idx = tid; idx < mfit * mfit; idx += kThreads) {
+                const int j = idx / mfit, k = idx - j * mfit;
+                ev.alpha[idx] = s.alpha[j * ld + k];
+            }
+            if (tid < mfit) ev.beta[tid] = s.beta[tid];
+            if (tid == 0) {
+                ev.chisq[0] = chisq;
+                ev.area[0] = s.scal[S_AREA];
+            }
+            return;
         }
-        if (tid < mfit) ev.beta[tid] = s.beta[tid];
-        if (tid == 0) {
-            ev.chisq[0] = chisq;
-            ev.area[0] = s.scal[S_AREA];
-        }
-        return;
     }
 
+    int cur = -1;  // batch: the object whose tables are loaded
     for (;;) {
         if (tid == 0) s.ctl[C_ITEM] = atomicAdd(queue, 1);
         __syncthreads();
         const int item = s.ctl[C_ITEM];
         if (item >= n_items) break;
-
-        // initial parameters (CudaCalculatePreparePole, Start.cu:4346-4418)
-        if (tid == 0) {
-            const FitItem it = items[item];
-            double *a = s.a;
-            a[0] = 0;
-            for (int k = 1; k <= nc; ++k) a[k] = __ldg(&o.cg_first[k - 1]);
-            const double period = 1.0 / (p.freq_start - (it.n_freq - 1) * p.freq_step);
-            a[nc + 1] = (kPi / 180) * 90 - (kPi / 180) * p.beta_pole[it.pole];
-            a[nc + 2] = (kPi / 180) * p.lambda_pole[it.pole];
-            a[nc + 3] = (24.0 * 2.0 * kPi) / period;
-            a[nc + 4] = p.par[0];
-            a[nc + 5] = p.par[1];
-            a[nc + 6] = p.par[2];
-            a[ma - 1] = p.lcl;
-            a[ma] = 1;
-            s.scal[S_ALAMDA] = -1;
-            s.scal[S_ITERDIFF] = 1e40;
-            s.scal[S_DEVOLD] = 1e30;
-            s.scal[S_DEVNEW] = 0;
-            s.scal[S_CHCK] = 0;
-            s.ctl[C_NITER] = 0;
-            s.ctl[C_STATUS] = 0;
-        }
-        __syncthreads();
-
-        for (;;) {
-            // convergence test (CudaCalculateIter1Begin, Start.cu:4421-4462)
-            if (tid == 0) {
-                const int niter = s.ctl[C_NITER];
-                s.ctl[C_GO] = ((niter < p.n_iter_max) && (s.scal[S_ITERDIFF] > p.iter_diff_max)) ||
-                              (niter < p.n_iter_min);
-            }
-            __syncthreads();
-            if (!s.ctl[C_GO]) break;
-            const bool first = s.scal[S_ALAMDA] < 0;
-            __syncthreads();
-            if (first) {
-                if (tid == 0) s.scal[S_ALAMDA] = p.alamda_start;
-                double oc = evaluate<NCP, MIXED>(o, p, s, s.a, s.alpha, s.beta, rows, cstat, perm, p.conw_r);
-                if (tid == 0) s.scal[S_OCHISQ] = oc;
-                for (int q = tid; q <= ma; q += kThreads) s.atry[q] = s.a[q];
-                __syncthreads();
-            }
-            // damped normal matrix and solve (mrqmin_1_end_opt)
-            const double ccc = 1 + s.scal[S_ALAMDA];
-            for (int idx = tid; idx < mfit * mfit; idx += kThreads) {
-                const int j = idx / mfit, k = idx - j * mfit;
-                const double v = s.alpha[j * ld + k];
-                s.covar[j * ld + k] = (j == k) ? v * ccc : v;
-            }
-            if (tid < mfit) s.da[tid] = s.beta[tid];
-            __syncthreads();
-            tmark(p, s, T_REST);
-            const int err = gauss_jordan(s, mfit);
-            tmark(p, s, T_SOLVE);
-            if (err == 0 || err == 2) {
-                if (tid < mfit) s.atry[s.fidx[tid]] = s.a[s.fidx[tid]] + s.da[tid];
-                if (err == 2 && tid == 0) s.ctl[C_STATUS] |= kStatusSingular;
-            }
-            __syncthreads();
-            const double chisq = evaluate<NCP, MIXED>(o, p, s, s.atry, s.covar, s.da, rows, cstat, perm, p.conw_r);
-            // accept / reject (mrqmin_2_end, Start.cu:300-392)
-            const bool accept = chisq < s.scal[S_OCHISQ];
-            __syncthreads();
-            if (accept) {
-                for (int idx = tid; idx < mfit * ld; idx += kThreads) s.alpha[idx] = s.covar[idx];
-                if (tid < mfit) s.beta[tid] = s.da[tid];
-                for (int q = tid; q <= ma; q += kThreads) s.a[q] = s.atry[q];
-            }
-            if (tid == 0) {
-                if (isnan(chisq)) s.ctl[C_STATUS] |= kStatusNanChisq;
-                if (accept) {
-                    s.scal[S_ALAMDA] *= p.alamda_incrr;
-                    s.scal[S_CHISQ] = chisq;
-                } else {
-                    s.scal[S_ALAMDA] = p.alamda_incr * s.scal[S_ALAMDA];
-                    s.scal[S_CHISQ] = s.scal[S_OCHISQ];
-                }
-                s.ctl[C_NITER] += 1;
-            }
-            __syncthreads();
-            // rms and convergence bookkeeping (CudaCalculateIter2, Start.cu:5129-5248)
-            const int niter = s.ctl[C_NITER];
-            const double ch = s.scal[S_CHISQ];
-            if (niter == 1 || ch < s.scal[S_OCHISQ]) {
-                __syncthreads();
-                const double area_sum = shape_areas(o, s, s.a);
-                double r[3] = {0, 0, 0};
-                for (int fi = tid; fi < o.n_fac; fi += kThreads) {
-                    const double4 fr = s.F[fi];
-                    r[0] += fr.w * fr.x;
-                    r[1] += fr.w * fr.y;
-                    r[2] += fr.w * fr.z;
-                }
-                block_sum<3>(r, s.red);
+        const FitItem it = items[item];
+        if constexpr (BATCH) {
+            const int k = it.pole >> kPoleBits;
+            if (k != cur) {
                 if (tid == 0) {
-                    s.scal[S_OCHISQ] = ch;
-                    s.scal[S_AREA] = area_sum;
-                    const double aa = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-                    const double rchisq = ch - aa * (p.conw_r_dev * p.conw_r_dev);
-                    const double dev_new = sqrt(rchisq / (o.n_points + 3 - 3));
-                    s.scal[S_DEVNEW] = dev_new;
-                    s.scal[S_CHCK] = sqrt(aa);
-                    const double diff = s.scal[S_DEVOLD] - dev_new;
-                    if (diff > 1e-10) {
-                        s.scal[S_ITERDIFF] = diff;
-                        s.scal[S_DEVOLD] = dev_new;
-                    }
+                    s_obj = objs[k];
+                    s_prm = prms[k];
                 }
+                __syncthreads();
+                for (int f = tid; f < s_obj.n_fac; f += kThreads) s.F[f] = ldg4(&s_obj.facet[f]);
+                if (tid < s_obj.mfit) s.fidx[tid] = __ldg(&s_obj.fidx[tid]);
+                __syncthreads();
+                cur = k;
             }
-            __syncthreads();
-        }
-
-        // per-fit result (CudaCalculateFinishPole, Start.cu:5056-5125)
-        if (tid == 0) {
-            double dd = s.scal[S_CHCK] * 100.0 * (1.0 / s.scal[S_AREA]);
-            if (isnan(dd)) dd = 1.0;
-            const double la = (180 / kPi) * s.a[nc + 2];
-            FitOut r;
-            r.dev = s.scal[S_DEVNEW];
-            r.dark = dd;
-            r.per = 2 * kPi / s.a[nc + 3];
-            r.lambda_deg = la + (la < 0 ? 360 : 0);
-            r.beta_deg = 90 - (180 / kPi) * s.a[nc + 1];
-            r.chisq = s.scal[S_CHISQ];
-            r.niter = s.ctl[C_NITER];
-            r.status = s.ctl[C_STATUS] | (s.ctl[C_TIMEOUT] ? kStatusTimeout : 0);
-            out[item] = r;
-            if (r.status) atomicOr(status, r.status);
-            if (p.phase_cycles) {
-                tmark(p, s, T_REST);
-                for (int q = 0; q < T_NPHASE; ++q) {
-                    atomicAdd(&p.phase_cycles[q], (unsigned long long)s.tclk[q]);
-                    s.tclk[q] = 0;
-                }
-            }
+            fit_one<NCP, MIXED>(s_obj, s_prm, s, it, item, out, rows, status);
+        } else {
+            fit_one<NCP, MIXED>(o, p, s, it, item, out, rows, status);
         }
         __syncthreads();
         if (s.ctl[C_TIMEOUT]) break;  // a bulk copy never completed: stop taking items
