@@ -37,6 +37,10 @@ def synth_text(kind: str, seed: int):
                                    sparse_curves=1, n_freq=3),
         # lmax 8, relative data only (87 fitted parameters)
         "lmax8rel": synth.SynthConfig(l_max=8, m_max=8, nrows=10, n_dense=5, dense_pts=(30, 40), n_freq=3),
+        # stop condition < 1: fits run until the rms improves by less than 0.005
+        # (at least 10, at most 60 iterations)
+        "conv": synth.SynthConfig(l_max=3, m_max=3, nrows=5, n_dense=8, dense_pts=(30, 40), n_freq=4,
+                                  stop_condition=0.005),
         # calibrated data only: no relative curve, no renormalisation
         "calonly": synth.SynthConfig(l_max=4, m_max=4, nrows=6, n_dense=0, n_sparse=150, sparse_curves=3, n_freq=3),
         # ragged: relative curves of 1 to 3 points beside one calibrated curve
