@@ -302,6 +302,11 @@ int32_t ps_n_coef(int32_t l_max, int32_t m_max);
 /* FP64 FMA throughput of the device in TFLOP/s (the compute roofline of the
    fit kernel; no reference counterpart). */
 ps_status ps_measure_fp64_peak(int32_t device, double *tflops);
+/* Test hook (no reference counterpart): one CTA waits, with the fit
+   kernel's bounded wait and a limit of `polls` polls, on a bulk-copy barrier
+   that nothing completes; *status = PS_DEVSTAT_TIMEOUT when the wait gave up
+   (0 if it had completed).  The context stays usable. */
+ps_status ps_probe_wait_timeout(int32_t polls, int32_t *status);
 /* Test hook: r[i] = the fit kernel's branch-free reciprocal of d[i], on the
    current device (no reference counterpart). */
 ps_status ps_probe_reciprocal(int32_t n, const double *d, double *r);

@@ -127,10 +127,11 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 }
 
 // Waits for the phase with the given parity to complete; gives up after
-// kWaitLimit polls and returns false (the caller records a timeout).
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity)
+// `limit` polls (kWaitLimit in the fit kernel) and returns false (the caller
+// records a timeout).
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity, unsigned limit = kWaitLimit)
 {
-    for (unsigned i = 0; i < kWaitLimit; ++i) {
+    for (unsigned i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"

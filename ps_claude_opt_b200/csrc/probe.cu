@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "devmath.cuh"
+#include "fit_kernel.cuh"
 #include "ps_b200.h"
 #include "util.h"
 
@@ -34,7 +35,34 @@ __global__ void rcp_probe(const double *d, double *r, int n)
     if (i < n) r[i] = psb::rcp_nr(d[i]);
 }
 
+// A bulk-copy barrier that nothing will ever complete: the fit kernel's
+// bounded wait on it must give up and report, leaving the context usable.
+__global__ void wait_probe(unsigned limit, int *status)
+{
+    __shared__ unsigned long long bar;
+    if (threadIdx.x == 0) psb::mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) status[0] = psb::mbar_wait(&bar, 0, limit) ? 0 : psb::kStatusTimeout;
+}
+
 }  // namespace
+
+extern "C" ps_status ps_probe_wait_timeout(int32_t polls, int32_t *status)
+{
+    if (polls < 1 || !status) return psb_fail(PS_ERR_ARG, "ps_probe_wait_timeout: bad arguments");
+    int *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(int));
+    if (e != cudaSuccess) return psb_fail_cuda(e, "cudaMalloc");
+    e = cudaMemset(d, 0xff, sizeof(int));
+    if (e == cudaSuccess) {
+        wait_probe<<<1, 32>>>((unsigned)polls, d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(status, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return psb_fail_cuda(e, "ps_probe_wait_timeout");
+    return PS_OK;
+}
 
 extern "C" ps_status ps_probe_reciprocal(int32_t n, const double *d, double *r)
 {

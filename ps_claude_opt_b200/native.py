@@ -21,6 +21,7 @@ PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 DEVSTAT_SINGULAR = 1
 DEVSTAT_NAN_CHISQ = 2
+DEVSTAT_TIMEOUT = 4
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -108,6 +109,7 @@ _SIGS = {
     "ps_n_coef": (C.c_int32, [C.c_int32, C.c_int32]),
     "ps_measure_fp64_peak": (C.c_int, [C.c_int32, _dp]),
     "ps_probe_reciprocal": (C.c_int, [C.c_int32, _dp, _dp]),
+    "ps_probe_wait_timeout": (C.c_int, [C.c_int32, _ip]),
     "ps_last_error": (C.c_char_p, []),
     "ps_version": (C.c_char_p, []),
 }
