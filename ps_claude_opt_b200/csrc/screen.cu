@@ -40,14 +40,31 @@ constexpr int kMaxScreenCurves = 256;
 constexpr int kGlobalFolds = 3;
 constexpr int kFeatures = kStats * kAggs + kGlobalFolds * kStats;
 
-// Per-curve statistics of one fold (lane 0 of a warp, bins in shared memory).
-__device__ void curve_stats(const float *cnt, const float *sum, const float *ssq, float *st)
+// Bin sums are fixed-point (2^-32 units) 64-bit integers: shared-memory
+// atomics on them add in any order to the same total, so the features -- and
+// the screen's choice of frequencies -- are the same on every run.
+constexpr double kFix = 4294967296.0;  // 2^32
+
+__device__ __forceinline__ void bin_add(unsigned long long *cnt, unsigned long long *sum, unsigned long long *ssq,
+                                        int b, float v)
 {
+    atomicAdd(&cnt[b], 1ull);
+    atomicAdd(&sum[b], (unsigned long long)__double2ll_rn((double)v * kFix));
+    atomicAdd(&ssq[b], (unsigned long long)__double2ll_rn((double)v * (double)v * kFix));
+}
+
+// Per-curve statistics of one fold (lane 0 of a warp, bins in shared memory).
+__device__ void curve_stats(const unsigned long long *cntb, const unsigned long long *sumb,
+                            const unsigned long long *ssqb, float *st)
+{
+    auto cnt = [&](int b) { return (double)cntb[b]; };
+    auto sum = [&](int b) { return (double)(long long)sumb[b] / kFix; };
+    auto ssq = [&](int b) { return (double)(long long)ssqb[b] / kFix; };
     double n = 0, s1 = 0, s2 = 0;
     for (int b = 0; b < kBins; ++b) {
-        n += cnt[b];
-        s1 += sum[b];
-        s2 += ssq[b];
+        n += cnt(b);
+        s1 += sum(b);
+        s2 += ssq(b);
     }
     const double total = s2 - (n > 0 ? s1 * s1 / n : 0.0);
     for (int lev = 0; lev < 4; ++lev) {  // B = 64 >> lev bins
@@ -56,9 +73,9 @@ __device__ void curve_stats(const float *cnt, const float *sum, const float *ssq
         for (int b = 0; b < kBins; b += w) {
             double c = 0, a = 0, q = 0;
             for (int i = 0; i < w; ++i) {
-                c += cnt[b + i];
-                a += sum[b + i];
-                q += ssq[b + i];
+                c += cnt(b + i);
+                a += sum(b + i);
+                q += ssq(b + i);
             }
             if (c > 0) within += q - a * a / c;
         }
@@ -67,9 +84,9 @@ __device__ void curve_stats(const float *cnt, const float *sum, const float *ssq
     // harmonics of the 32-bin mean curve (empty bins left out)
     double re[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
     for (int b = 0; b < 32; ++b) {
-        const double c = cnt[2 * b] + cnt[2 * b + 1];
+        const double c = cnt(2 * b) + cnt(2 * b + 1);
         if (c <= 0) continue;
-        const double m = (sum[2 * b] + sum[2 * b + 1]) / c;
+        const double m = (sum(2 * b) + sum(2 * b + 1)) / c;
         for (int k = 0; k < 4; ++k) {
             double sn, cs;
             sincospi((double)(2 * (k + 1) * b) / 32.0, &sn, &cs);
@@ -92,26 +109,23 @@ __global__ void __launch_bounds__(kFeatThreads) features_kernel(const double *ti
                                                                  const double *freqs, int n_freq, double t_mid,
                                                                  float *out)
 {
-    __shared__ float bins[kFeatWarps][3][kBins];
+    __shared__ unsigned long long bins[kFeatWarps][3][kBins];
     __shared__ float cst[kStats][kMaxScreenCurves];
     __shared__ float cw[kMaxScreenCurves];
     const int f = blockIdx.x;
     if (f >= n_freq) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const double fr = freqs[f];
-    float *cnt = bins[warp][0], *sum = bins[warp][1], *ssq = bins[warp][2];
+    unsigned long long *cnt = bins[warp][0], *sum = bins[warp][1], *ssq = bins[warp][2];
     for (int c = warp; c < n_curves; c += kFeatWarps) {
-        for (int b = lane; b < kBins; b += 32) cnt[b] = sum[b] = ssq[b] = 0.0f;
+        for (int b = lane; b < kBins; b += 32) cnt[b] = sum[b] = ssq[b] = 0ull;
         __syncwarp();
         const int p0 = cstart[c], p1 = cstart[c + 1];
         for (int i = p0 + lane; i < p1; i += 32) {
             const double ph = tim[i] * fr;
             const double frac = ph - floor(ph);
             const int b = min(kBins - 1, max(0, (int)(frac * kBins)));
-            const float v = y[i];
-            atomicAdd(&cnt[b], 1.0f);
-            atomicAdd(&sum[b], v);
-            atomicAdd(&ssq[b], v * v);
+            bin_add(cnt, sum, ssq, b, y[i]);
         }
         __syncwarp();
         if (lane == 0) {
@@ -127,7 +141,7 @@ __global__ void __launch_bounds__(kFeatThreads) features_kernel(const double *ti
     // warp 0 adds the eight partial histograms and lane 0 takes the stats
     const int n_pts = cstart[n_curves];
     for (int fold = 0; fold < kGlobalFolds; ++fold) {
-        for (int b = lane; b < kBins; b += 32) cnt[b] = sum[b] = ssq[b] = 0.0f;
+        for (int b = lane; b < kBins; b += 32) cnt[b] = sum[b] = ssq[b] = 0ull;
         __syncwarp();
         for (int i = threadIdx.x; i < n_pts; i += kFeatThreads) {
             const double t = tim[i];
@@ -135,10 +149,7 @@ __global__ void __launch_bounds__(kFeatThreads) features_kernel(const double *ti
             const double ph = t * fr;
             const double frac = ph - floor(ph);
             const int b = min(kBins - 1, max(0, (int)(frac * kBins)));
-            const float v = y[i];
-            atomicAdd(&cnt[b], 1.0f);
-            atomicAdd(&sum[b], v);
-            atomicAdd(&ssq[b], v * v);
+            bin_add(cnt, sum, ssq, b, y[i]);
         }
         __syncthreads();
         if (warp == 0) {

@@ -22,6 +22,8 @@ def test_features_match_cpu_restatement():
     assert got.shape == (len(freqs), 88)
     assert np.all(np.isfinite(got))
     assert np.max(np.abs(got - ref)) < 1e-4
+    # fixed-point bin sums: the same features on every run
+    assert np.array_equal(screen.features(obj, freqs), got)
 
 
 def _bf16(rng, *shape):
