@@ -310,6 +310,12 @@ ps_status ps_probe_wait_timeout(int32_t polls, int32_t *status);
 /* Test hook: r[i] = the fit kernel's branch-free reciprocal of d[i], on the
    current device (no reference counterpart). */
 ps_status ps_probe_reciprocal(int32_t n, const double *d, double *r);
+/* Test hook: the fit kernel's full-pivot Gauss-Jordan solve (the solve of
+   mrqmin_1_end_opt, Start.cu:2880-3006) of the row-major n x n system a x = b,
+   1 <= n <= 89, in one CTA on the current device; x = the solve's da, *err =
+   its error code (0, 1 pivot bookkeeping, 2 zero pivot: x then holds the
+   partial solution the fit uses). */
+ps_status ps_probe_solve(int32_t n, const double *a, const double *b, double *x, int32_t *err);
 
 const char *ps_last_error(void);
 const char *ps_version(void);

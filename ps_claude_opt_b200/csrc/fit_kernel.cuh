@@ -40,7 +40,7 @@ constexpr unsigned kWaitLimit = 1u << 24;  // bounded mbarrier waits
 
 // LM scalar slots in shared memory
 enum { S_ALAMDA, S_CHISQ, S_OCHISQ, S_ITERDIFF, S_DEVOLD, S_DEVNEW, S_CHCK, S_AREA, S_TRIAL, S_PIVINV, S_NSCAL };
-enum { C_ITEM, C_NITER, C_STATUS, C_ERR, C_IROW, C_ICOL, C_GO, C_ACCEPT, C_TIMEOUT,
+enum { C_ITEM, C_NITER, C_STATUS, C_GJROW0, C_GO, C_TIMEOUT,
        C_YUSE,                       // [kStages] completed uses of each chunk buffer
        C_REL = C_YUSE + kStages,     // [kStages] warps done with the chunk in each buffer
        C_TUSE = C_REL + kStages,     // [2] completed uses of each J^T W J tile buffer
@@ -87,9 +87,7 @@ struct Sh {
     double *red;      // [kWarps * 4]
     double *inv;      // [40] per-evaluation invariants
     double *scal;     // [S_NSCAL]
-    double *colbuf;   // [kMaxFit]
     int *fidx;        // [kMaxFit]
-    int *ipiv;        // [kMaxFit]
     int *ctl;         // [C_NCTL]
     int ld, mfp, tr;
 };
@@ -215,9 +213,7 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, int 
     void *red = take(sizeof(double) * kWarps * 4);
     void *inv = take(sizeof(double) * 40);
     void *scal = take(sizeof(double) * S_NSCAL);
-    void *colbuf = take(sizeof(double) * kMaxFit);
     void *fidx = take(sizeof(int) * kMaxFit);
-    void *ipiv = take(sizeof(int) * kMaxFit);
     void *ctl = take(sizeof(int) * C_NCTL);
     void *mbar = take(sizeof(unsigned long long) * kStages);
     void *tbar = take(sizeof(unsigned long long) * 2);
@@ -241,7 +237,7 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, int 
         s->rdy = (double *)rdy; s->rw = (double *)rw;
         s->rcoef = (double *)rcoef; s->rsub = (double *)rsub; s->rcur = (int *)rcur;
         s->red = (double *)red; s->inv = (double *)inv; s->scal = (double *)scal;
-        s->colbuf = (double *)colbuf; s->fidx = (int *)fidx; s->ipiv = (int *)ipiv; s->ctl = (int *)ctl;
+        s->fidx = (int *)fidx; s->ctl = (int *)ctl;
         s->mbar = (unsigned long long *)mbar; s->tbar = (unsigned long long *)tbar;
         s->tclk = (long long *)tclk; s->hist = (int *)hist;
         s->ccoef = (double *)ccoef; s->crave = (double *)crave; s->cst = (double *)cst;
@@ -1382,150 +1378,276 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
 // ---------------------------------------------------------------- LM step
 
 // Full-pivot Gauss-Jordan on covar (n x n, stride ld) and b = da
-// (mrqmin_1_end_opt, Start.cu:2880-3006).  The pivot is the maximum |a| over
-// unpivoted rows and columns; among equal values the last one in row-major
-// order wins, as in the serial scan: threads (64 row slots x 4 column phases)
-// keep a local candidate (|a|, j*n + k) and the CTA reduces on it, which
-// selects exactly that element.  The candidate search for pivot i+1 runs
-// inside the elimination of pivot i, on the values just written.  The inverse
-// is not needed, so already-pivoted columns are left stale.  Returns the
-// reference's error code: 0, 1 (pivot bookkeeping) or 2 (zero pivot).  All
-// threads must call it.
+// (mrqmin_1_end_opt, Start.cu:2880-3006), one CTA barrier per pivot.
+//
+// The pivot is the maximum |a| over unpivoted rows and columns; among equal
+// values the last one in row-major order wins, as in the serial scan: every
+// candidate carries (|a|, logical row * n + column) and the CTA takes the
+// lexicographic maximum (NaN is never a candidate).  The candidate search for
+// pivot i+1 runs inside the elimination of pivot i, on the values just
+// written.
+//
+// Thread (rsub, csub) owns row slots rsub + 64 r and columns csub + 4 j.  A
+// row swap only swaps the logical labels of two slots (kept in registers), so
+// rows never move.  The pivot row is not scaled when it is chosen: every
+// reader forms the scaled value pivot_row[l] * pivinv itself (the same
+// rounding as a stored product), and the row's owners apply the scale when
+// they next touch it, in the following elimination.  ipiv lives in register
+// bit masks, alike in all threads.  The rounding of every stored value equals
+// the serial algorithm's; the inverse is not needed, so already-pivoted
+// columns are left stale.  Returns the reference's error code: 0, 1 (pivot
+// bookkeeping) or 2 (zero pivot).  All threads must call it.
+struct __align__(16) GjCand {
+    double v;  // |a| of the warp's best candidate, -1 if it has none
+    int key;   // logical row * n + column
+    int slot;  // row slot, bit 31 = bookkeeping fault seen
+};
+
+__device__ __forceinline__ bool gj_mask_bit(unsigned w0, unsigned w1, unsigned w2, int c)
+{
+    const unsigned w = c < 32 ? w0 : (c < 64 ? w1 : w2);
+    return (w >> (c & 31)) & 1u;
+}
+
+// kMaxN: the largest n the caller passes (row slots and columns per thread
+// are sized for it).
+template <int kMaxN>
 static __device__ int gauss_jordan(const Sh &s, int n)
 {
+    constexpr int kSlots = kThreads / 4;
+    constexpr int kRowsPer = (kMaxN + kSlots - 1) / kSlots;
+    constexpr int kColsPer = (kMaxN + 3) / 4;
+    static_assert(kMaxN <= kMaxFit && kMaxFit <= 96 && kRowsPer <= 2, "pivot masks are 32-bit words");
+    static_assert(kMaxFit * kMaxFit < (1 << 13) && kMaxFit < (1 << 7), "key division by multiply and shift");
+    static_assert(sizeof(GjCand) * 2 * kWarps <= sizeof(double) * kWarps * 4, "candidate buffers in red");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int ld = s.ld;
-    const int rsub = tid >> 2, csub = tid & 3;
+    const int ld = s.ld, rsub = tid >> 2, csub = tid & 3;
+    const unsigned ndiv = ((1u << 20) + n - 1) / n;  // key / n == (key * ndiv) >> 20 for key < n * n
     double *A = s.covar, *b = s.da;
-    int *ipiv = s.ipiv;
-    if (tid < n) ipiv[tid] = 0;
-    __syncthreads();
-    double big = -1.0;
-    int key = 0;
-    for (int j = rsub; j < n; j += kThreads / 4) {
-        const double *row = A + j * ld;
-        for (int k = csub; k < n; k += 4) {
-            const double t = fabs(row[k]);
-            if (t >= big) {
-                big = t;
-                key = j * n + k;
+    GjCand *cand_buf = reinterpret_cast<GjCand *>(s.red);
+
+    int lab[kRowsPer];
+#pragma unroll
+    for (int r = 0; r < kRowsPer; ++r) lab[r] = rsub + kSlots * r;
+    unsigned g1a = 0, g1b = 0, g1c = 0;  // columns with ipiv >= 1
+    unsigned g2a = 0, g2b = 0, g2c = 0;  // columns with ipiv >= 2
+    unsigned c1 = 0, c2 = 0;             // the same for this thread's columns, bit j = column csub + 4 j
+    int pend = -1;                       // slot of the previous pivot row (scale pending)
+    double pend_inv = 1.0;
+
+    double bv = -1.0;  // the thread's best candidate
+    int bkey = 0, bslot = 0;
+    bool bad = false;
+    // a row's best (the last of equal values, columns being visited in order)
+    // joins the thread's candidate
+    auto cand = [&](double big, int j, int L, int slot) {
+        const int key = L * n + csub + 4 * j;
+        if (big > bv || (big == bv && big >= 0.0 && key > bkey)) {
+            bv = big;
+            bkey = key;
+            bslot = slot;
+        }
+    };
+    auto row_open = [&](int L) {  // ipiv[L] != 1
+        return !(gj_mask_bit(g1a, g1b, g1c, L) && !gj_mask_bit(g2a, g2b, g2c, L));
+    };
+
+#pragma unroll
+    for (int r = 0; r < kRowsPer; ++r) {
+        const int ll = rsub + kSlots * r;
+        if (ll < n) {
+            const double *row = A + ll * ld;
+            double big = -1.0;
+            int bj = 0;
+#pragma unroll
+            for (int j = 0; j < kColsPer; ++j) {
+                const int l = csub + 4 * j;
+                if (l < n) {
+                    const double t = fabs(row[l]);
+                    if (t >= big) {
+                        big = t;
+                        bj = j;
+                    }
+                }
             }
+            cand(big, bj, ll, ll);
         }
     }
-    bool bad = false;
+
     int err = 0;
     for (int i = 0; i < n; ++i) {
+        {
+            // warp maximum of (|a|, key): |a| >= 0 orders like its bits, -1 below all
+            const int hi = __double2hiint(bv);
+            const unsigned lo = (unsigned)__double2loint(bv);
+            const int mh = __reduce_max_sync(0xffffffffu, hi);
+            const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+            const bool top = hi == mh && lo == ml;
+            const unsigned mk = __reduce_max_sync(0xffffffffu, top ? (unsigned)bkey : 0u);
+            const unsigned who = __ballot_sync(0xffffffffu, top && (unsigned)bkey == mk);
+            const int wslot = __shfl_sync(0xffffffffu, bslot, __ffs(who) - 1);
+            const unsigned wbad = __reduce_or_sync(0xffffffffu, bad ? 1u : 0u);
+            if (lane == 0) {
+                GjCand c;
+                c.v = __hiloint2double(mh, (int)ml);
+                c.key = (int)mk;
+                c.slot = wslot | (int)(wbad << 31);
+                cand_buf[(i & 1) * kWarps + warp] = c;
+            }
+        }
+        __syncthreads();
+        int irow, icol, P;
+        bool none;
+        {
+            const GjCand *e = cand_buf + (i & 1) * kWarps;
+            GjCand c[kWarps];
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const double ob = __shfl_xor_sync(0xffffffffu, big, off);
-            const int ok = __shfl_xor_sync(0xffffffffu, key, off);
-            if (ob > big || (ob == big && ok > key)) {
-                big = ob;
-                key = ok;
+            for (int w = 0; w < kWarps; ++w) c[w] = e[w];
+            double vm = c[0].v;
+            int any = c[0].slot;
+#pragma unroll
+            for (int w = 1; w < kWarps; ++w) {
+                vm = fmax(vm, c[w].v);
+                any |= c[w].slot;
             }
-        }
-        const bool wbad = __any_sync(0xffffffffu, bad);
-        if (lane == 0) {
-            s.red[warp * 4 + 0] = big;
-            s.red[warp * 4 + 1] = (double)key;
-            s.red[warp * 4 + 2] = wbad ? 1.0 : 0.0;
-        }
-        __syncthreads();
-        double bb = s.red[0];
-        int bkey = (int)s.red[1];
-        bool anybad = s.red[2] != 0.0;
-        for (int w = 1; w < kWarps; ++w) {
-            const double ob = s.red[w * 4];
-            const int ok = (int)s.red[w * 4 + 1];
-            anybad = anybad || s.red[w * 4 + 2] != 0.0;
-            if (ob > bb || (ob == bb && ok > bkey)) {
-                bb = ob;
-                bkey = ok;
+            if (any < 0) {
+                err = 1;
+                break;
             }
+            int km = -1;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) km = max(km, c[w].v == vm ? c[w].key : -1);
+            int sl = 0;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) sl |= (c[w].v == vm && c[w].key == km) ? c[w].slot : 0;
+            none = vm < 0.0;
+            irow = (int)(((unsigned)km * ndiv) >> 20);
+            icol = km - irow * n;
+            P = sl;
         }
-        if (anybad) {
-            err = 1;
-            break;
-        }
-        if (bb < 0.0) bkey = 0;  // nothing but NaN left: the serial scan's (0, 0)
-        const int irow = bkey / n, icol = bkey - irow * n;
-        const double piv = A[irow * ld + icol];
-        double row_r = 0.0, row_c = 0.0, colv = 0.0;
-        if (tid < n) {
-            row_r = A[irow * ld + tid];
-            row_c = A[icol * ld + tid];
-            colv = (tid == irow) ? A[icol * ld + icol] : A[tid * ld + icol];
-        }
-        const double b_r = b[irow], b_c = b[icol];
-        __syncthreads();
-        if (piv == 0.0) {
-            err = 2;
-            // the reference swaps the rows before it meets the zero pivot
-            if (tid < n) {
-                A[irow * ld + tid] = row_c;
-                A[icol * ld + tid] = row_r;
-            }
-            if (tid == 0) {
-                b[irow] = b_c;
-                b[icol] = b_r;
+        if (none) {
+            // nothing but NaN left: the serial scan's (0, 0).  Row 0 may be
+            // the pending row, so scale that first, then find row 0's slot.
+            irow = icol = 0;
+#pragma unroll
+            for (int r = 0; r < kRowsPer; ++r) {
+                const int ll = rsub + kSlots * r;
+                if (ll >= n) continue;
+                if (ll == pend) {
+                    double *row = A + ll * ld;
+#pragma unroll
+                    for (int j = 0; j < kColsPer; ++j) {
+                        const int l = csub + 4 * j;
+                        if (l < n && !((c1 >> j) & 1u)) row[l] = __dmul_rn(row[l], pend_inv);
+                    }
+                    if (csub == 0) b[ll] = __dmul_rn(b[ll], pend_inv);
+                }
+                if (lab[r] == 0 && csub == 0) s.ctl[C_GJROW0] = ll;
             }
             __syncthreads();
+            P = s.ctl[C_GJROW0];
+            pend = -1;
+        }
+        // the swap of rows irow and icol
+#pragma unroll
+        for (int r = 0; r < kRowsPer; ++r) lab[r] = lab[r] == irow ? icol : (lab[r] == icol ? irow : lab[r]);
+        // P is an open row, never the pending one (that one is closed, or a
+        // bookkeeping fault ended the solve above, or the NaN branch scaled it)
+        const double piv = A[P * ld + icol];
+        if (piv == 0.0) {
+            err = 2;
             break;
         }
         const double pivinv = 1.0 / piv;
-        if (tid < n) {
-            A[irow * ld + tid] = row_c;
-            A[icol * ld + tid] = (tid == icol) ? pivinv : row_r * pivinv;
-            s.colbuf[tid] = colv;
+        const double bs = __dmul_rn(b[P], pivinv);
+        // ipiv[icol] += 1
+        {
+            const unsigned m = 1u << (icol & 31);
+            if (icol < 32) {
+                if (g1a & m) g2a |= m;
+                g1a |= m;
+            } else if (icol < 64) {
+                if (g1b & m) g2b |= m;
+                g1b |= m;
+            } else {
+                if (g1c & m) g2c |= m;
+                g1c |= m;
+            }
+            if ((icol & 3) == csub) {
+                const unsigned mj = 1u << (icol >> 2);
+                if (c1 & mj) c2 |= mj;
+                c1 |= mj;
+            }
         }
-        if (tid == 0) {
-            ipiv[icol] += 1;
-            b[irow] = b_c;
-            b[icol] = b_r * pivinv;
-        }
-        __syncthreads();
         // eliminate (only unpivoted columns feed later pivots and b) and look
         // for the next pivot among unpivoted rows and columns
-        big = -1.0;
-        key = 0;
+        bv = -1.0;
+        bkey = 0;
+        bslot = 0;
         bad = false;
-        const double *prow = A + icol * ld;
-        for (int ll = rsub; ll < n; ll += kThreads / 4) {
-            const bool open_row = ipiv[ll] != 1;
-            double *row = A + ll * ld;
-            if (ll == icol) {
-                if (open_row)  // only after a bookkeeping fault: keep the serial checks
-                    for (int l = csub; l < n; l += 4) {
-                        const int il = ipiv[l];
-                        if (il == 0) {
-                            const double t = fabs(row[l]);
-                            if (t >= big) { big = t; key = ll * n + l; }
-                        } else if (il > 1) {
-                            bad = true;
+        const double *__restrict__ prow = A + P * ld;
+#pragma unroll 1
+        for (int r = 0; r < kRowsPer; ++r) {
+            const int ll = rsub + kSlots * r;
+            if (ll >= n) continue;
+            const int L = r == 0 ? lab[0] : lab[kRowsPer - 1];
+            const bool open = row_open(L);
+            double *__restrict__ row = A + ll * ld;
+            if (open && c2) bad = true;  // a column with ipiv > 1 in an open row
+            double big = -1.0;
+            int bj = 0;
+            if (ll == P) {
+                if (open) {  // only after a bookkeeping fault: keep the serial checks
+#pragma unroll
+                    for (int j = 0; j < kColsPer; ++j) {
+                        const int l = csub + 4 * j;
+                        if (l < n && !((c1 >> j) & 1u)) {
+                            const double t = fabs(__dmul_rn(row[l], pivinv));
+                            if (t >= big) {
+                                big = t;
+                                bj = j;
+                            }
                         }
                     }
+                    cand(big, bj, L, ll);
+                }
                 continue;
             }
-            const double cb = s.colbuf[ll];
-            for (int l = csub; l < n; l += 4) {
-                const int il = ipiv[l];
-                if (il == 0) {
-                    const double v = row[l] - prow[l] * cb;
+            // x * 1.0 == x exactly: rows other than the pending one pass unscaled
+            const double rs = ll == pend ? pend_inv : 1.0;
+            const double cb = __dmul_rn(row[icol], rs);
+#pragma unroll
+            for (int j = 0; j < kColsPer; ++j) {
+                const int l = csub + 4 * j;
+                if (l < n && !((c1 >> j) & 1u)) {
+                    const double v = __fma_rn(-__dmul_rn(prow[l], pivinv), cb, __dmul_rn(row[l], rs));
                     row[l] = v;
-                    if (open_row) {
-                        const double t = fabs(v);
-                        if (t >= big) {
-                            big = t;
-                            key = ll * n + l;
-                        }
+                    const double t = fabs(v);
+                    if (t >= big) {
+                        big = t;
+                        bj = j;
                     }
-                } else if (il > 1 && open_row) {
-                    bad = true;
                 }
             }
+            if (open) cand(big, bj, L, ll);
+            if (csub == 0) b[ll] = __fma_rn(-bs, cb, __dmul_rn(b[ll], rs));
         }
-        const double bi = b[icol];
-        if (tid < n && tid != icol) b[tid] -= bi * s.colbuf[tid];
+        pend = P;
+        pend_inv = pivinv;
+    }
+    // b back to logical order, the pending scale applied
+    double bo[kRowsPer];
+#pragma unroll
+    for (int r = 0; r < kRowsPer; ++r) {
+        const int ll = rsub + kSlots * r;
+        bo[r] = 0.0;
+        if (ll < n && csub == 0) bo[r] = ll == pend ? __dmul_rn(b[ll], pend_inv) : b[ll];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kRowsPer; ++r) {
+        const int ll = rsub + kSlots * r;
+        if (ll < n && csub == 0) b[lab[r]] = bo[r];
     }
     __syncthreads();
     return err;
@@ -1597,7 +1719,8 @@ __device__ __forceinline__ void fit_one(const DevObject &o, const DevParams &p, 
         if (tid < mfit) s.da[tid] = s.beta[tid];
         __syncthreads();
         tmark(p, s, T_REST);
-        const int err = gauss_jordan(s, mfit);
+        // mfit <= ma = n_coef + 8 <= NCP + 8 (and < kMaxFit)
+        const int err = gauss_jordan<(NCP + 8 < kMaxFit ? NCP + 8 : kMaxFit)>(s, mfit);
         tmark(p, s, T_SOLVE);
         if (err == 0 || err == 2) {
             if (tid < mfit) s.atry[s.fidx[tid]] = s.a[s.fidx[tid]] + s.da[tid];

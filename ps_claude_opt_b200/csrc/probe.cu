@@ -45,7 +45,62 @@ __global__ void wait_probe(unsigned limit, int *status)
     if (threadIdx.x == 0) status[0] = psb::mbar_wait(&bar, 0, limit) ? 0 : psb::kStatusTimeout;
 }
 
+// The fit kernel's damped solve on one n x n system (one CTA, the kernel's
+// shared-memory layout for covar, da, red and ctl).
+__global__ void __launch_bounds__(psb::kThreads) solve_probe(const double *a, const double *b, int n, double *x,
+                                                             int *err)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int ld = psb::fit_ld(n);
+    psb::Sh s{};
+    double *covar = reinterpret_cast<double *>(smem);
+    double *da = covar + (size_t)n * ld + (n * ld & 1);
+    double *red = da + psb::kMaxFit;
+    int *ctl = reinterpret_cast<int *>(red + psb::kWarps * 4);
+    s.covar = covar;
+    s.da = da;
+    s.red = red;
+    s.ctl = ctl;
+    s.ld = ld;
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) covar[(idx / n) * ld + idx % n] = a[idx];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) da[j] = b[j];
+    __syncthreads();
+    const int e = n <= 64 ? psb::gauss_jordan<64>(s, n) : psb::gauss_jordan<psb::kMaxFit>(s, n);
+    for (int j = threadIdx.x; j < n; j += blockDim.x) x[j] = da[j];
+    if (threadIdx.x == 0) err[0] = e;
+}
+
+size_t solve_probe_smem(int n)
+{
+    const size_t ld = psb::fit_ld(n);
+    return sizeof(double) * ((size_t)n * ld + 1 + psb::kMaxFit + psb::kWarps * 4) + sizeof(int) * psb::C_NCTL;
+}
+
 }  // namespace
+
+extern "C" ps_status ps_probe_solve(int32_t n, const double *a, const double *b, double *x, int32_t *err)
+{
+    if (n < 1 || n > psb::kMaxFit - 1 || !a || !b || !x || !err)
+        return psb_fail(PS_ERR_ARG, "ps_probe_solve: bad arguments");
+    double *d = nullptr;
+    const size_t nn = (size_t)n * n;
+    cudaError_t e = cudaMalloc(&d, sizeof(double) * (nn + 2 * (size_t)n) + sizeof(int) * 2);
+    if (e != cudaSuccess) return psb_fail_cuda(e, "cudaMalloc");
+    int *derr = reinterpret_cast<int *>(d + nn + 2 * n);
+    const size_t smem = solve_probe_smem(n);
+    e = cudaFuncSetAttribute(solve_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) e = cudaMemcpy(d, a, sizeof(double) * nn, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + nn, b, sizeof(double) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        solve_probe<<<1, psb::kThreads, smem>>>(d, d + nn, n, d + nn + n, derr);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(x, d + nn + n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(err, derr, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return psb_fail_cuda(e, "ps_probe_solve");
+    return PS_OK;
+}
 
 extern "C" ps_status ps_probe_wait_timeout(int32_t polls, int32_t *status)
 {

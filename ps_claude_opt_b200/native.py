@@ -110,6 +110,7 @@ _SIGS = {
     "ps_measure_fp64_peak": (C.c_int, [C.c_int32, _dp]),
     "ps_probe_reciprocal": (C.c_int, [C.c_int32, _dp, _dp]),
     "ps_probe_wait_timeout": (C.c_int, [C.c_int32, _ip]),
+    "ps_probe_solve": (C.c_int, [C.c_int32, _dp, _dp, _dp, _ip]),
     "ps_last_error": (C.c_char_p, []),
     "ps_version": (C.c_char_p, []),
 }
@@ -172,6 +173,19 @@ def probe_reciprocal(d):
     r = np.zeros_like(d)
     _check(lib().ps_probe_reciprocal(len(d), _p(d), _p(r)))
     return r
+
+
+def probe_solve(a, b):
+    """The fit kernel's Gauss-Jordan solve of a x = b on the GPU: (err, x)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    n = b.shape[0]
+    if a.shape != (n, n):
+        raise ValueError("probe_solve: a must be n x n")
+    x = np.zeros(n)
+    err = np.zeros(1, dtype=np.int32)
+    _check(lib().ps_probe_solve(n, _p(a), _p(b), _p(x), _p(err, C.c_int32)))
+    return int(err[0]), x
 
 
 class Engine:
