@@ -21,6 +21,7 @@
 // update, rms and convergence test) follows Start.cu:300-392, 2838-3021,
 // 4421-4462, 5129-5248 with Numerical-Recipes ia compaction.
 #pragma once
+#include <climits>
 #include <cuda_runtime.h>
 
 #include "devmath.cuh"
@@ -153,7 +154,10 @@ __device__ __forceinline__ void tmark(const DevParams &p, const Sh &s, int phase
     }
 }
 
-__host__ __device__ inline int fit_ld(int mfit) { return mfit | 1; }
+// Row stride of alpha and covar: 4 mod 8 doubles, so the 8 rows x 4
+// consecutive columns a warp touches in the solve's elimination spread evenly
+// over the shared-memory banks.
+__host__ __device__ inline int fit_ld(int mfit) { return mfit + ((4 - mfit) & 7); }
 // Row stride of the J^T W J staging tiles: the augmented width mfit + 1
 // rounded to whole 8-column MMA blocks, then to 4 mod 16 doubles so the
 // 8x4 / 4x8 fragment loads of a half-warp hit 16 distinct 8-byte banks.
@@ -1409,6 +1413,21 @@ __device__ __forceinline__ bool gj_mask_bit(unsigned w0, unsigned w1, unsigned w
     return (w >> (c & 31)) & 1u;
 }
 
+// Lane holding the warp's maximum of (value, key), value given as its high
+// word (signed: values >= 0 order like their bits, -1 below all) and low
+// word; among equal values the largest key.  Nearly always the high words
+// alone decide.
+__device__ __forceinline__ int gj_argmax(int hi, unsigned lo, int key)
+{
+    const int mh = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned tie = __ballot_sync(0xffffffffu, hi == mh);
+    if (__popc(tie) == 1) return __ffs(tie) - 1;
+    const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+    const bool top = hi == mh && lo == ml;
+    const unsigned mk = __reduce_max_sync(0xffffffffu, top ? (unsigned)key : 0u);
+    return __ffs(__ballot_sync(0xffffffffu, top && (unsigned)key == mk)) - 1;
+}
+
 // kMaxN: the largest n the caller passes (row slots and columns per thread
 // are sized for it).
 template <int kMaxN>
@@ -1420,6 +1439,7 @@ static __device__ int gauss_jordan(const Sh &s, int n)
     static_assert(kMaxN <= kMaxFit && kMaxFit <= 96 && kRowsPer <= 2, "pivot masks are 32-bit words");
     static_assert(kMaxFit * kMaxFit < (1 << 13) && kMaxFit < (1 << 7), "key division by multiply and shift");
     static_assert(sizeof(GjCand) * 2 * kWarps <= sizeof(double) * kWarps * 4, "candidate buffers in red");
+    static_assert(kWarps <= 32 && (kWarps & (kWarps - 1)) == 0, "one lane per warp candidate");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ld = s.ld, rsub = tid >> 2, csub = tid & 3;
     const unsigned ndiv = ((1u << 20) + n - 1) / n;  // key / n == (key * ndiv) >> 20 for key < n * n
@@ -1477,21 +1497,17 @@ static __device__ int gauss_jordan(const Sh &s, int n)
     int err = 0;
     for (int i = 0; i < n; ++i) {
         {
-            // warp maximum of (|a|, key): |a| >= 0 orders like its bits, -1 below all
             const int hi = __double2hiint(bv);
-            const unsigned lo = (unsigned)__double2loint(bv);
-            const int mh = __reduce_max_sync(0xffffffffu, hi);
-            const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
-            const bool top = hi == mh && lo == ml;
-            const unsigned mk = __reduce_max_sync(0xffffffffu, top ? (unsigned)bkey : 0u);
-            const unsigned who = __ballot_sync(0xffffffffu, top && (unsigned)bkey == mk);
-            const int wslot = __shfl_sync(0xffffffffu, bslot, __ffs(who) - 1);
-            const unsigned wbad = __reduce_or_sync(0xffffffffu, bad ? 1u : 0u);
+            const int src = gj_argmax(hi, (unsigned)__double2loint(bv), bkey);
+            const double wv = __shfl_sync(0xffffffffu, bv, src);
+            const int wkey = __shfl_sync(0xffffffffu, bkey, src);
+            const int wslot = __shfl_sync(0xffffffffu, bslot, src);
+            const bool wbad = __any_sync(0xffffffffu, bad);
             if (lane == 0) {
                 GjCand c;
-                c.v = __hiloint2double(mh, (int)ml);
-                c.key = (int)mk;
-                c.slot = wslot | (int)(wbad << 31);
+                c.v = wv;
+                c.key = wkey;
+                c.slot = wslot | (wbad ? (int)0x80000000u : 0);
                 cand_buf[(i & 1) * kWarps + warp] = c;
             }
         }
@@ -1499,31 +1515,21 @@ static __device__ int gauss_jordan(const Sh &s, int n)
         int irow, icol, P;
         bool none;
         {
-            const GjCand *e = cand_buf + (i & 1) * kWarps;
-            GjCand c[kWarps];
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) c[w] = e[w];
-            double vm = c[0].v;
-            int any = c[0].slot;
-#pragma unroll
-            for (int w = 1; w < kWarps; ++w) {
-                vm = fmax(vm, c[w].v);
-                any |= c[w].slot;
-            }
-            if (any < 0) {
+            // every warp combines the warps' candidates alike, lane w < kWarps
+            // holding warp w's
+            const GjCand c = cand_buf[(i & 1) * kWarps + (lane & (kWarps - 1))];
+            if (__any_sync(0xffffffffu, c.slot < 0)) {
                 err = 1;
                 break;
             }
-            int km = -1;
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) km = max(km, c[w].v == vm ? c[w].key : -1);
-            int sl = 0;
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) sl |= (c[w].v == vm && c[w].key == km) ? c[w].slot : 0;
+            const int hi = lane < kWarps ? __double2hiint(c.v) : INT_MIN;
+            const int src = gj_argmax(hi, (unsigned)__double2loint(c.v), c.key);
+            const double vm = __shfl_sync(0xffffffffu, c.v, src);
+            const int km = __shfl_sync(0xffffffffu, c.key, src);
+            P = __shfl_sync(0xffffffffu, c.slot, src);
             none = vm < 0.0;
             irow = (int)(((unsigned)km * ndiv) >> 20);
             icol = km - irow * n;
-            P = sl;
         }
         if (none) {
             // nothing but NaN left: the serial scan's (0, 0).  Row 0 may be
