@@ -1215,21 +1215,21 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
                     w = rec.y;
                 }
                 const double *dav = cstat + (size_t)max(cur, 0) * CS;
-                const double *rrow = rb + rr * RS;
+                const double *rrow = rb + rr * RS;  // inside the tile buffer even past nrows
+                const bool rel = cur >= 0;
                 double fa[8], fb[8];
+                // no branch around the loads (fit column clamped, row kept in the
+                // buffer), so the eight gathers are in flight together; selects
+                // zero what lies outside the tile or the matrix
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     const int j = 8 * q + jl;
-                    double v = 0.0;
-                    if (valid && q < acc.nb) {
-                        if (j < mfit) {
-                            const int col = s.fidx[j] - 1;
-                            const double raw = rrow[col];
-                            v = (cur >= 0) ? coef * (raw - sub * dav[col]) : raw;
-                        } else if (j == mfit) {
-                            v = dy;
-                        }
-                    }
+                    const int col = s.fidx[min(j, mfit - 1)] - 1;
+                    const double raw = rrow[col];
+                    const double dv = rel ? dav[col] : 0.0;
+                    double v = rel ? coef * (raw - sub * dv) : raw;
+                    v = j < mfit ? v : (j == mfit ? dy : 0.0);
+                    v = valid ? v : 0.0;
                     fb[q] = v;
                     fa[q] = v * w;
                 }
@@ -1290,18 +1290,17 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
             const double *dav = cstat + (size_t)max(cur, 0) * CS;
             const double *rrow = rb + rr * RS;
             double *trow = s.T + rr * mfp, *twrow = s.TW + rr * mfp;
+            const bool rel = cur >= 0;
             double v[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < 4; ++u) {  // branch-free gathers, as in the k-slice form
                 const int j = lane + 32 * u;
-                v[u] = 0.0;
-                if (valid && j < mfit) {
-                    const int col = s.fidx[j] - 1;
-                    const double raw = rrow[col];
-                    v[u] = (cur >= 0) ? coef * (raw - sub * dav[col]) : raw;
-                } else if (valid && j == mfit) {
-                    v[u] = dy;
-                }
+                const int col = s.fidx[min(j, mfit - 1)] - 1;
+                const double raw = rrow[col];
+                const double dv = rel ? dav[col] : 0.0;
+                v[u] = rel ? coef * (raw - sub * dv) : raw;
+                v[u] = j < mfit ? v[u] : (j == mfit ? dy : 0.0);
+                v[u] = valid ? v[u] : 0.0;
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
