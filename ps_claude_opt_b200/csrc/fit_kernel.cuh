@@ -1132,19 +1132,20 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
         if (!o.curve_rel[c]) continue;
         const int p0 = o.curve_start[c], p1 = o.curve_start[c + 1];
         // columns lane, lane + 32, lane + 64 (ma + 1 <= 90); the rows come from
-        // HBM, so each step issues the loads of 8 points before adding them
+        // HBM, so each step issues the loads of 16 points before adding them
+        constexpr int kStep = 16;
         double sum[3] = {0, 0, 0};
-        for (int q0 = p0; q0 < p1; q0 += 8) {
-            double v[8][3];
+        for (int q0 = p0; q0 < p1; q0 += kStep) {
+            double v[kStep][3];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
+            for (int u = 0; u < kStep; ++u) {
                 const bool ok = q0 + u < p1;
                 const double *r = rows + (size_t)(ok ? q0 + u : p0) * RS;
 #pragma unroll
                 for (int j = 0; j < 3; ++j) v[u][j] = (ok && lane + 32 * j <= ma) ? r[lane + 32 * j] : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
+            for (int u = 0; u < kStep; ++u)
 #pragma unroll
                 for (int j = 0; j < 3; ++j) sum[j] += v[u][j];
         }
