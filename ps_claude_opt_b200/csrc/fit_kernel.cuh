@@ -1193,6 +1193,9 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
         // barrier; the last warp done with a buffer refills it
         const int rr = 4 * warp + (lane & 3);
         const int jl = lane >> 2;
+        int colq[8];  // raw-row column of this lane's fit column 8 q + jl (clamped)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) colq[q] = s.fidx[min(8 * q + jl, mfit - 1)] - 1;
         for (int t = 0; t < ntile; ++t) {
             const int b = t & 1, r0 = t * TR, nrows = min(TR, np - r0);
             tmark(p, s, T_TILES);
@@ -1225,7 +1228,7 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     const int j = 8 * q + jl;
-                    const int col = s.fidx[min(j, mfit - 1)] - 1;
+                    const int col = colq[q];
                     const double raw = rrow[col];
                     const double dv = rel ? dav[col] : 0.0;
                     double v = rel ? coef * (raw - sub * dv) : raw;
