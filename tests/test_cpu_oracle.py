@@ -59,6 +59,28 @@ def test_gauss_jordan_solves():
     assert rc == 2
 
 
+def test_gauss_jordan_known_answers():
+    """The oracle's solve equals the exact rational solve, bit for bit, on
+    tie-heavy systems whose elimination is exact (pivot order and tie-break
+    included), and on rank-deficient ones its zero-pivot partial solution."""
+    import numpy as np
+
+    import solve_cases
+
+    cases = solve_cases.exact_cases(np.random.default_rng(2024))
+    assert len(cases) >= 20
+    for A, b, (rerr, rx) in cases:
+        rc, x = oracle.gauss_solve(A, b)
+        assert rc == rerr == 0
+        np.testing.assert_array_equal(x, np.array([float(v) for v in rx]))
+    cases = solve_cases.rank_deficient_cases(np.random.default_rng(7))
+    assert len(cases) >= 8
+    for A, b, (rerr, rx) in cases:
+        rc, x = oracle.gauss_solve(A, b)
+        assert rc == rerr == 2
+        np.testing.assert_array_equal(x, np.array([float(v) for v in rx]))
+
+
 def _step(obj, a, p):
     # the rotation rate multiplies times of ~1000 days: a finite-difference step
     # of 1e-6 already turns the body by ~1e-3 rad and crosses facet terminators
