@@ -127,28 +127,37 @@ def cpu_baseline(obj, n_fits, freq_offset=1):
     return n_fits / dt, cores, dt
 
 
+def workload_name(obj):
+    return ("production object: lmax 6 (49 coeffs), 512 facets, %d points (%d curves, 400 calibrated), "
+            "%d frequencies x 10 poles, 50 LM iterations" % (obj.n_points, obj.n_curves, obj.grid.n_max))
+
+
 def reference_arm(args, rank, world):
+    """The reference's fit has no runnable CPU form and its GPU form needs
+    BOINC: the CPU port of the same algorithm (the oracle) on all host cores
+    stands in.  Under torchrun rank 0 alone runs it; the others exit."""
     if rank != 0:
         return
     obj, _ = workload()
     cores = os.cpu_count() or 1
     per_step = max(8, cores)
-    cpu_baseline(obj, min(per_step, 16))   # warm-up: page in, spin up threads
+    freq_at = lambda s: 1 + s * (per_step // 10 + 1)  # noqa: E731
+    for s in range(max(1, args.warmup)):  # untimed: page in, spin up threads
+        cpu_baseline(obj, per_step, freq_offset=freq_at(s))
     times = []
     for s in range(args.steps):
-        rate, _, dt = cpu_baseline(obj, per_step, freq_offset=1 + s * (per_step // 10 + 1))
+        rate, _, dt = cpu_baseline(obj, per_step, freq_offset=freq_at(args.warmup + s))
         times.append(dt)
     total = sum(times)
     value = per_step * args.steps / total
     n_obj = obj.grid.n_max * 10
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": 0,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator; no public dataset ships with the reference)",
-        "config": {"workload": "production object: lmax 6, 512 facets, %d points, %d frequencies x 10 poles, "
-                               "50 LM iterations" % (obj.n_points, obj.grid.n_max),
-                   "sample": "%d fits per step" % per_step},
+        "config": {"workload": workload_name(obj), "sample": "%d fits per step" % per_step,
+                   "parallelism": "host threads (CPU port of the fit on %d cores; no GPU)" % cores},
         "s_per_object": n_obj / value,
         "cpu_baseline": {"value": value, "unit": "fits/s", "cores": cores, "kind": "port",
                          "sample": "%d fits x %d steps of the production object on %d threads" %
@@ -354,9 +363,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator; no public dataset ships with the reference)",
-            "config": {"workload": "production object: lmax 6 (49 coeffs), 512 facets, %d points (%d curves, "
-                                   "400 calibrated), %d frequencies x 10 poles, 50 LM iterations" %
-                                   (obj.n_points, obj.n_curves, n_max),
+            "config": {"workload": workload_name(obj),
                        "fits_per_step_per_gpu": n_fits, "ctas_per_sm": ctas,
                        "l2": "256 MB buffer written between timed launches; per-launch scratch %.0f MB > L2" %
                              (ctas * nsm * (obj.n_points * (obj.ma + 2) + obj.n_curves * (obj.ma + 3)) * 8 / 1e6),
