@@ -1341,16 +1341,33 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
             ym[2] += fr.w * fr.z;
         }
         block_sum<3>(ym, s.red);
-        // raw derivative d ym_i / d a_k for shape coefficient k = tid
+        // raw derivative d ym_i / d a_k for shape coefficient k = tid: groups
+        // of nc threads take consecutive facet ranges, their partial sums
+        // (staged in the idle tile buffer) are added in group order
         double dk[3] = {0, 0, 0};
-        if (tid < nc) {
-            for (int fi = 0; fi < nf; ++fi) {
-                const double4 fr = s.F[fi];
-                const double y = __ldg(o.ysh + (size_t)fi * o.ncp + tid);
-                dk[0] += (fr.w * fr.x) * y;
-                dk[1] += (fr.w * fr.y) * y;
-                dk[2] += (fr.w * fr.z) * y;
+        {
+            const int ngrp = max(1, min(kThreads / nc, (s.tr * mfp) / (3 * nc)));
+            const int per = (nf + ngrp - 1) / ngrp;
+            const int grp = tid / nc, k = tid - grp * nc;
+            if (grp < ngrp) {
+                double pk[3] = {0, 0, 0};
+                const int fe = min(nf, (grp + 1) * per);
+                for (int fi = grp * per; fi < fe; ++fi) {
+                    const double4 fr = s.F[fi];
+                    const double y = __ldg(o.ysh + (size_t)fi * o.ncp + k);
+                    pk[0] += (fr.w * fr.x) * y;
+                    pk[1] += (fr.w * fr.y) * y;
+                    pk[2] += (fr.w * fr.z) * y;
+                }
+#pragma unroll
+                for (int i = 0; i < 3; ++i) s.T[(grp * 3 + i) * nc + k] = pk[i];
             }
+            __syncthreads();
+            if (tid < nc)
+                for (int g2 = 0; g2 < ngrp; ++g2)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) dk[i] += s.T[(g2 * 3 + i) * nc + tid];
+            __syncthreads();
         }
         const double wps = conw_r * conw_r;
         for (int idx = tid; idx < kTile * mfp; idx += kThreads) {
