@@ -22,6 +22,7 @@
 // 4421-4462, 5129-5248 with Numerical-Recipes ia compaction.
 #pragma once
 #include <climits>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "devmath.cuh"
@@ -1190,63 +1191,51 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
         // k-slice mode: warp w owns rows 4w..4w+3 of every tile and builds its
         // MMA fragments straight from the raw rows in shared memory (lane row
         // 4w + lane%4, fit column 8q + lane/4), so the tile loop needs no CTA
-        // barrier; the last warp done with a buffer refills it
+        // barrier; the last warp done with a buffer refills it.  Software
+        // pipelined: the fragments of tile t+1 are built (and its buffer
+        // released) in the same branch-free stretch of code that issues the
+        // MMAs of tile t, so the gathers overlap the tensor-core work.
         const int rr = 4 * warp + (lane & 3);
         const int jl = lane >> 2;
         int colq[8];  // raw-row column of this lane's fit column 8 q + jl (clamped)
 #pragma unroll
         for (int q = 0; q < 8; ++q) colq[q] = s.fidx[min(8 * q + jl, mfit - 1)] - 1;
-        for (int t = 0; t < ntile; ++t) {
-            const int b = t & 1, r0 = t * TR, nrows = min(TR, np - r0);
-            tmark(p, s, T_TILES);
+        auto wait_tile = [&](int t) {
+            const int b = t & 1;
             if (!mbar_wait(&s.tbar[b], (uint32_t)((s.ctl[C_TUSE + b] + (t >> 1)) & 1))) timeout = true;
-            tmark(p, s, T_TWAIT);
-            if (4 * warp < nrows) {
-                const double *rb = s.raw + (size_t)b * TR * RS;
-                const bool valid = rr < nrows;
-                double dy = 0.0, w = 0.0, coef = 0.0, sub = 0.0;
-                int cur = -1;
-                if (valid) {
-                    const double4 rec = s.recb[b * TR + rr];
-                    double ymod = rb[rr * RS + ma];
-                    if (rec.w != 0.0) {
-                        cur = (int)rec.z;
-                        coef = s.ccoef[cur];
-                        sub = ymod * s.crave[cur];
-                        ymod = coef * ymod;
-                    }
-                    dy = rec.x - ymod;
-                    w = rec.y;
-                }
-                const double *dav = cstat + (size_t)max(cur, 0) * CS;
-                const double *rrow = rb + rr * RS;  // inside the tile buffer even past nrows
-                const bool rel = cur >= 0;
-                double fa[8], fb[8];
-                // no branch around the loads (fit column clamped, row kept in the
-                // buffer), so the eight gathers are in flight together; selects
-                // zero what lies outside the tile or the matrix
+        };
+        // rows past the tile's end (and whole warps past it) read stale but
+        // in-buffer data and contribute exact zeros
+        auto build = [&](int t, double (&fa)[8], double (&fb)[8]) {
+            const int b = t & 1, nrows = min(TR, np - t * TR);
+            const double *rb = s.raw + (size_t)b * TR * RS;
+            const bool valid = rr < nrows;
+            const double4 rec = s.recb[b * TR + rr];
+            const double ymod0 = rb[rr * RS + ma];
+            const bool rel = valid && rec.w != 0.0;
+            const int cur = rel ? (int)rec.z : 0;
+            const double coef = rel ? s.ccoef[cur] : 0.0;
+            const double sub = rel ? ymod0 * s.crave[cur] : 0.0;
+            const double ymod = rel ? coef * ymod0 : ymod0;
+            const double dy = valid ? rec.x - ymod : 0.0;
+            const double w = valid ? rec.y : 0.0;
+            const double *dav = cstat + (size_t)cur * CS;
+            const double *rrow = rb + rr * RS;
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const int j = 8 * q + jl;
-                    const int col = colq[q];
-                    const double raw = rrow[col];
-                    const double dv = rel ? dav[col] : 0.0;
-                    double v = rel ? coef * (raw - sub * dv) : raw;
-                    v = j < mfit ? v : (j == mfit ? dy : 0.0);
-                    v = valid ? v : 0.0;
-                    fb[q] = v;
-                    fa[q] = v * w;
-                }
-#pragma unroll
-                for (int bj = 0; bj < 8; ++bj)
-#pragma unroll
-                    for (int bk = 0; bk <= bj; ++bk)
-                        if (bj < acc.nb) {
-                            const int i = bj * (bj + 1) / 2 + bk;
-                            dmma_8x8x4(acc.c[i][0], acc.c[i][1], fa[bj], fb[bk]);
-                        }
+            for (int q = 0; q < 8; ++q) {
+                const int j = 8 * q + jl;
+                const int col = colq[q];
+                const double raw = rrow[col];
+                const double dv = rel ? dav[col] : 0.0;
+                double v = rel ? coef * (raw - sub * dv) : raw;
+                v = j < mfit ? v : (j == mfit ? dy : 0.0);
+                v = valid ? v : 0.0;
+                fb[q] = v;
+                fa[q] = v * w;
             }
-            tmark(p, s, T_TSYRK);
+        };
+        auto release = [&](int t) {
+            const int b = t & 1;
             __syncwarp();
             if (lane == 0) {
                 __threadfence_block();
@@ -1255,7 +1244,42 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
                     if (t + 2 < ntile) tissue(t + 2);
                 }
             }
-        }
+        };
+        auto run = [&](auto full8) {
+            constexpr bool kFull = decltype(full8)::value;
+            auto mmas = [&](const double (&fa)[8], const double (&fb)[8]) {
+#pragma unroll
+                for (int bj = 0; bj < 8; ++bj)
+#pragma unroll
+                    for (int bk = 0; bk <= bj; ++bk)
+                        if (kFull || bj < acc.nb) {
+                            const int i = bj * (bj + 1) / 2 + bk;
+                            dmma_8x8x4(acc.c[i][0], acc.c[i][1], fa[bj], fb[bk]);
+                        }
+            };
+            double fa[8], fb[8], ga[8], gb[8];
+            wait_tile(0);
+            build(0, fa, fb);
+            release(0);
+            for (int t = 0; t + 1 < ntile; ++t) {
+                wait_tile(t + 1);
+                build(t + 1, ga, gb);
+                mmas(fa, fb);
+                release(t + 1);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    fa[q] = ga[q];
+                    fb[q] = gb[q];
+                }
+            }
+            mmas(fa, fb);
+        };
+        tmark(p, s, T_TILES);
+        if (acc.nb == 8)
+            run(std::true_type{});
+        else
+            run(std::false_type{});
+        tmark(p, s, T_TSYRK);
         __syncthreads();
     } else {
     for (int t = 0; t < ntile; ++t) {
