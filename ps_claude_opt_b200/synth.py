@@ -45,6 +45,16 @@ class SynthConfig:
 C1 = SynthConfig()
 C2 = SynthConfig(l_max=6, m_max=6, nrows=8, n_dense=40, dense_pts=(50, 120), n_sparse=400,
                  sparse_curves=2, period_range=(2.0, 100.0), n_freq=5000)
+# The production object with relative lightcurves only (the form the
+# reference's GPU code evaluates correctly: it skips the brightness of
+# calibrated curves) on 200 trial frequencies around the true period.
+C2_REL = dataclasses.replace(C2, n_sparse=0, period_range=None, n_freq=200, period_step_coef=3.0)
+
+# Trailing "lc# weight" pair appended to inputs run by the reference app: its
+# weight loop (period_search_BOINC.cpp:524-533) prints weightLc[lcNumber]
+# after the final failed read, so lcNumber must have been set once.  Weight 1
+# for curve 1 equals the default and changes nothing.
+NEUTRAL_WEIGHT_LINE = "1 1.0\n"
 
 
 def _basis(l_max, m_max, theta, phi):
@@ -245,3 +255,26 @@ def write(cfg: SynthConfig, seed: int, path: str):
     with open(path, "w") as f:
         f.write(text)
     return truth
+
+
+def config3_object(i: int, seed0: int = 1000003 * 3):
+    """Object i of the batched workload: points log-uniform in 300..19 900
+    (relative curves of equal length, at most 199 of them -- with the
+    pseudo-curve the reference's MAX_LC of 200), lmax = mmax in {4, 6, 8},
+    nrows in {6, 8, 10}, trial-frequency count log-uniform in 500..20 000
+    around the true period, stop condition 0.005 (fits run until the rms
+    improves by less than that: ragged iteration counts).  Returns
+    (SynthConfig, seed)."""
+    rng = np.random.default_rng(seed0 + i)
+    n_pts = int(round(math.exp(rng.uniform(math.log(300), math.log(19900)))))
+    lmax = int(rng.choice([4, 6, 8]))
+    nrows = int(rng.choice([6, 8, 10]))
+    n_freq = int(round(math.exp(rng.uniform(math.log(500), math.log(20000)))))
+    n_curves = min(199, max(5, n_pts // 80))
+    per = max(1, n_pts // n_curves)
+    cfg = SynthConfig(l_max=lmax, m_max=lmax, nrows=nrows, n_dense=n_curves, dense_pts=(per, per),
+                      n_freq=n_freq, stop_condition=0.005, n_iter_min=10)
+    return cfg, seed0 + i
+
+
+C3_OBJECTS = 64
