@@ -29,8 +29,11 @@
 //                    tensor-core shape derivatives, FP64 elsewhere)
 //     --screen MODEL fit only the frequencies a trained screening network
 //                    ranks first (the top 3.4 % with one neighbour on either
-//                    side, plus a 2 % audit sample); one output line per
-//                    fitted frequency, in frequency order; no checkpoints
+//                    side, plus a 2 % audit sample), widen around a best line
+//                    at the edge of a fitted run, and fall back to the whole
+//                    grid when the audit sample contradicts the ranking; one
+//                    output line per fitted frequency, in frequency order; no
+//                    checkpoints
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -187,24 +190,27 @@ bool read_model(const std::string &path, std::vector<int32_t> &sizes, std::vecto
     return ok;
 }
 
-// The frequencies (0-based) a screened scan fits: the lowest-scoring
-// `top` share with `halo` neighbours each side, plus an `audit` share of the
-// rest drawn by a partial Fisher-Yates shuffle from a 64-bit linear
-// congruential generator (the Python screen draws the same sample).
-std::vector<int> screen_select(const std::vector<float> &score, double top, int halo, double audit, uint64_t seed)
+// The frequencies (0-based) a screened scan fits first: the core -- the
+// lowest-scoring `top` share with `halo` neighbours each side -- and an
+// `audit` share of the rest drawn by a partial Fisher-Yates shuffle from a
+// 64-bit linear congruential generator (ps_claude_opt_b200.screen.select_parts
+// draws the same sample).  core[i] / audit[i] mark the two sets.
+void screen_parts(const std::vector<float> &score, double top, int halo, double audit, uint64_t seed,
+                  std::vector<char> &core, std::vector<char> &aud)
 {
     const int n = (int)score.size();
     std::vector<int> order(n);
     for (int i = 0; i < n; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return score[a] < score[b]; });
     const int k = std::max(1, (int)std::nearbyint(top * n));
-    std::vector<char> chosen(n, 0);
+    core.assign(n, 0);
+    aud.assign(n, 0);
     for (int r = 0; r < k; ++r)
         for (int d = -halo; d <= halo; ++d)
-            if (order[r] + d >= 0 && order[r] + d < n) chosen[order[r] + d] = 1;
+            if (order[r] + d >= 0 && order[r] + d < n) core[order[r] + d] = 1;
     std::vector<int> rest;
     for (int i = 0; i < n; ++i)
-        if (!chosen[i]) rest.push_back(i);
+        if (!core[i]) rest.push_back(i);
     const int na = std::min((int)rest.size(), std::max(1, (int)std::nearbyint(audit * n)));
     uint64_t x = seed * 2654435761ull + 1ull;
     for (int j = 0; j < na; ++j) {
@@ -212,12 +218,39 @@ std::vector<int> screen_select(const std::vector<float> &score, double top, int 
         const uint64_t r = x >> 33;
         const int pick = j + (int)(r % (uint64_t)(rest.size() - j));
         std::swap(rest[j], rest[pick]);
-        chosen[rest[j]] = 1;
+        aud[rest[j]] = 1;
     }
-    std::vector<int> out;
-    for (int i = 0; i < n; ++i)
-        if (chosen[i]) out.push_back(i);
-    return out;
+}
+
+// Control flow of a screened scan (ps_claude_opt_b200.screen.plan_scan):
+// fit the core and the audit sample; while the best line has an unfitted
+// neighbour, fit kEdge more frequencies each side of it (at most
+// kMaxExpansions times, then fall back); if an audit frequency farther than
+// kEdge from the best line comes within kAuditMargin (relative) of its rms,
+// fall back.  Falling back fits every remaining frequency, which makes the
+// output the full scan's.
+constexpr double kAuditMargin = 0.10;
+constexpr int kEdge = 2;
+constexpr int kMaxExpansions = 8;
+
+struct ScreenedScan {
+    std::vector<ps_line> line;   // per frequency (valid where fitted)
+    std::vector<char> fitted;
+    int initial = 0, expansions = 0;
+    bool fallback = false;
+    const char *reason = "";
+};
+
+int best_fitted(const ScreenedScan &sc)
+{
+    int b = -1;
+    double br = INFINITY;
+    for (size_t i = 0; i < sc.line.size(); ++i)
+        if (sc.fitted[i] && sc.line[i].rms < br) {   // NaN never wins; the first minimum wins ties
+            b = (int)i;
+            br = sc.line[i].rms;
+        }
+    return b;
 }
 
 int fail(const char *what)
@@ -326,34 +359,93 @@ int main(int argc, char **argv)
             ps_gpu_unprepare(h);
             return fail("screen");
         }
-        const std::vector<int> sel = screen_select(score, 0.034, 1, 0.02, 0);
-        std::vector<int32_t> nf, pl;
-        for (int f : sel)
-            for (int p = 0; p < PS_N_POLES; ++p) {
-                nf.push_back(f + 1);
-                pl.push_back(p);
-            }
-        std::vector<ps_fit_result> res(nf.size());
+        std::vector<char> core, aud;
+        screen_parts(score, 0.034, 1, 0.02, 0, core, aud);
         if (ps_gpu_configure(h, obj.freq_start, obj.freq_step, obj.stop_condition, obj.n_iter_min, conw_r, conw_r,
                              obj.n_points, obj.ia.data(), ia_par, obj.cg_first.data(), obj.sig.data(),
-                             obj.sigr2.data(), obj.n_fac, obj.brightness.data(), &curves, &shape) != PS_OK ||
-            ps_gpu_fit_items(h, (int32_t)nf.size(), nf.data(), pl.data(), res.data()) != PS_OK) {
+                             obj.sigr2.data(), obj.n_fac, obj.brightness.data(), &curves, &shape) != PS_OK) {
             std::fclose(out);
             ps_gpu_unprepare(h);
             return fail("screened scan");
         }
-        for (size_t q = 0; q < sel.size(); ++q) {
-            const ps_fit_result *r = &res[q * PS_N_POLES];
-            int best = -1;  // NaN-safe, earliest pole wins ties (start_CUDA.cu:1200-1229)
-            for (int p = 0; p < PS_N_POLES; ++p)
-                if (best < 0 || (!std::isnan(r[p].dev) && !(r[p].dev >= r[best].dev))) best = p;
-            const ps_fit_result &b = r[best];
-            const ps_line l{24 * b.per, b.dev, b.dev * b.dev * obj.n_points,
-                            sel[q] == 0 ? conw_r * obj.escl * obj.escl : b.dark, b.lambda_deg, b.beta_deg};
-            print_line(out, l);
+        ScreenedScan sc;
+        sc.line.resize(n_last);
+        sc.fitted.assign(n_last, 0);
+        // fits the unfitted frequencies among [lo, hi] whose mask is set
+        auto fit = [&](int lo, int hi, const std::vector<char> *mask) {
+            std::vector<int> sel;
+            for (int f = std::max(0, lo); f <= std::min(n_last - 1, hi); ++f)
+                if (!sc.fitted[f] && (!mask || (*mask)[f])) sel.push_back(f);
+            if (sel.empty()) return true;
+            std::vector<int32_t> nf, pl;
+            for (int f : sel)
+                for (int p = 0; p < PS_N_POLES; ++p) {
+                    nf.push_back(f + 1);
+                    pl.push_back(p);
+                }
+            std::vector<ps_fit_result> res(nf.size());
+            if (ps_gpu_fit_items(h, (int32_t)nf.size(), nf.data(), pl.data(), res.data()) != PS_OK) return false;
+            for (size_t q = 0; q < sel.size(); ++q) {
+                const ps_fit_result *r = &res[q * PS_N_POLES];
+                int best = -1;  // NaN-safe, earliest pole wins ties (start_CUDA.cu:1200-1229)
+                for (int p = 0; p < PS_N_POLES; ++p)
+                    if (best < 0 || (!std::isnan(r[p].dev) && !(r[p].dev >= r[best].dev))) best = p;
+                const ps_fit_result &b = r[best];
+                const int f = sel[q];
+                sc.line[f] = ps_line{24 * b.per, b.dev, b.dev * b.dev * obj.n_points,
+                                     f == 0 ? conw_r * obj.escl * obj.escl : b.dark, b.lambda_deg, b.beta_deg};
+                sc.fitted[f] = 1;
+            }
+            return true;
+        };
+        std::vector<char> first(n_last);
+        for (int f = 0; f < n_last; ++f) first[f] = core[f] || aud[f];
+        bool ok = fit(0, n_last - 1, &first);
+        for (int f = 0; f < n_last; ++f) sc.initial += sc.fitted[f];
+        while (ok) {
+            const int b = best_fitted(sc);
+            if (b < 0) {
+                sc.fallback = true;
+                sc.reason = "edge";
+                break;
+            }
+            const bool open = (b > 0 && !sc.fitted[b - 1]) || (b + 1 < n_last && !sc.fitted[b + 1]);
+            if (!open) break;
+            if (sc.expansions >= kMaxExpansions) {
+                sc.fallback = true;
+                sc.reason = "edge";
+                break;
+            }
+            ok = fit(b - kEdge, b + kEdge, nullptr);
+            ++sc.expansions;
         }
+        if (ok && !sc.fallback) {
+            const int b = best_fitted(sc);
+            for (int a = 0; a < n_last; ++a)
+                if (aud[a] && std::abs(a - b) > kEdge && sc.line[a].rms <= sc.line[b].rms * (1.0 + kAuditMargin)) {
+                    sc.fallback = true;
+                    sc.reason = "audit";
+                    break;
+                }
+        }
+        if (ok && sc.fallback) ok = fit(0, n_last - 1, nullptr);
+        if (!ok) {
+            std::fclose(out);
+            ps_gpu_unprepare(h);
+            return fail("screened scan");
+        }
+        int n_fit = 0;
+        for (int f = 0; f < n_last; ++f)
+            if (sc.fitted[f]) {
+                print_line(out, sc.line[f]);
+                ++n_fit;
+            }
         std::fclose(out);
-        std::fprintf(stderr, "period_search: screened scan fitted %zu of %d frequencies\n", sel.size(), n_last);
+        std::fprintf(stderr,
+                     "period_search: screened scan fitted %d of %d frequencies (first selection %d, %d edge "
+                     "expansions%s%s)\n",
+                     n_fit, n_last, sc.initial, sc.expansions, sc.fallback ? ", fell back to the full grid: " : "",
+                     sc.reason);
         ps_gpu_unprepare(h);
         return 0;
     }

@@ -203,12 +203,17 @@ def _lcg_uniform(seed, n):
     return out
 
 
-def select(pred, top=0.034, halo=1, audit=0.02, seed=0):
-    """Frequency indices (0-based) to fit: the `top` share with the lowest
-    predicted rms, each with `halo` neighbours on either side (an LM minimum
-    in frequency is a few grid steps wide, finer than the folded features
-    resolve), plus an `audit` share drawn uniformly from the rest.  The
-    defaults fit at most 12.2 % of the grid."""
+AUDIT_MARGIN = 0.10     # an audit line within 10 % of the screened best rms (the validator's rms envelope)
+EDGE_WIDTH = 2          # frequencies fitted on each side of a best line that sits at the edge of a fitted run
+MAX_EXPANSIONS = 8      # edge expansions before the scan falls back to the full grid
+
+
+def select_parts(pred, top=0.034, halo=1, audit=0.02, seed=0):
+    """(core, audit) frequency index sets (0-based) of a screened scan: the
+    `top` share with the lowest predicted rms, each with `halo` neighbours on
+    either side (an LM minimum in frequency is a few grid steps wide, finer
+    than the folded features resolve), and an `audit` share drawn uniformly
+    from the rest."""
     n = len(pred)
     k = max(1, int(round(top * n)))
     order = np.argsort(np.asarray(pred), kind="stable")
@@ -223,34 +228,141 @@ def select(pred, top=0.034, halo=1, audit=0.02, seed=0):
     for j, r in enumerate(_lcg_uniform(seed, na)):
         pick = j + r % (len(rest) - j)
         rest[j], rest[pick] = rest[pick], rest[j]
-    chosen.update(rest[:na])
-    return np.array(sorted(chosen), dtype=np.int64)
+    return chosen, set(rest[:na])
 
 
-def screened_scan(obj, net, conw_r, top=0.034, halo=1, audit=0.02, seed=0, device=0,
-                  precision=native.PRECISION_FP64):
-    """Fits only the screened frequencies (after the convexity-weight search,
-    whose conw_r is passed in).  Returns (frequency indices 1-based, lines,
-    per-fit results)."""
-    pred = net.predict(normalise(features(obj, frequencies(obj), device)))
-    idx = select(pred, top, halo, audit, seed) + 1
-    nf = np.repeat(idx, native.N_POLES).astype(np.int32)
-    pl = np.tile(np.arange(native.N_POLES), len(idx)).astype(np.int32)
-    with native.Engine(obj, device) as eng:
-        eng.set_precision(precision)
-        eng.configure(conw_r=conw_r)
-        res, niter, status = eng.fit_items(nf, pl)
-    res = res.reshape(len(idx), native.N_POLES, 6)
+def select(pred, top=0.034, halo=1, audit=0.02, seed=0):
+    """Frequency indices (0-based, sorted) a screened scan fits first: the
+    core and the audit sample of select_parts.  The defaults fit at most
+    12.2 % of the grid."""
+    core, aud = select_parts(pred, top, halo, audit, seed)
+    return np.array(sorted(core | aud), dtype=np.int64)
+
+
+class Plan:
+    """Outcome of a screened scan: the frequencies fitted (0-based, sorted),
+    their rms, and how the scan got there."""
+
+    def __init__(self, n):
+        self.n = n
+        self.rms = {}            # frequency -> best rms over the poles (NaN kept)
+        self.initial = 0         # frequencies of the first selection
+        self.expansions = 0      # edge expansions
+        self.fallback = False    # the whole grid was fitted
+        self.reason = ""         # why it fell back: "audit" or "edge"
+
+    @property
+    def fitted(self):
+        return sorted(self.rms)
+
+    def best(self):
+        """Lowest-rms fitted frequency (NaN never wins; the first minimum wins ties)."""
+        b, br = -1, np.inf
+        for i in self.fitted:
+            r = self.rms[i]
+            if r < br:
+                b, br = i, r
+        return b
+
+
+def plan_scan(pred, fit, top=0.034, halo=1, audit=0.02, seed=0, margin=AUDIT_MARGIN, edge=EDGE_WIDTH,
+              max_expansions=MAX_EXPANSIONS):
+    """The screened scan's control flow, independent of the device.
+
+    fit(indices) fits the given 0-based frequencies (all poles) and returns
+    each one's best rms.  Steps:
+      1. fit the core (top-ranked share with halo) and the audit sample;
+      2. while the best line sits at the edge of a fitted run (a neighbour is
+         unfitted), fit `edge` more frequencies on each side of it -- at most
+         `max_expansions` times, then fall back;
+      3. judge by the audit sample: if an audit frequency away from the best
+         line's neighbourhood comes within `margin` (relative) of the best
+         rms, the network's ranking is not trustworthy for this object and
+         the scan falls back;
+      4. on fallback, fit every remaining frequency: the result is then the
+         full scan's.
+    Returns a Plan."""
+    n = len(pred)
+    plan = Plan(n)
+    core, aud = select_parts(pred, top, halo, audit, seed)
+
+    def run(idx):
+        idx = sorted(i for i in set(idx) if 0 <= i < n and i not in plan.rms)
+        if idx:
+            for i, r in zip(idx, fit(np.array(idx, dtype=np.int64))):
+                plan.rms[i] = float(r)
+
+    run(core | aud)
+    plan.initial = len(plan.rms)
+    while True:
+        b = plan.best()
+        if b < 0:
+            plan.fallback, plan.reason = True, "edge"
+            break
+        need = [j for j in (b - 1, b + 1) if 0 <= j < n and j not in plan.rms]
+        if not need:
+            break
+        if plan.expansions >= max_expansions:
+            plan.fallback, plan.reason = True, "edge"
+            break
+        run(range(b - edge, b + edge + 1))
+        plan.expansions += 1
+    if not plan.fallback:
+        b = plan.best()
+        br = plan.rms[b]
+        for a in aud:
+            if abs(a - b) > edge and plan.rms.get(a, np.inf) <= br * (1.0 + margin):
+                plan.fallback, plan.reason = True, "audit"
+                break
+    if plan.fallback:
+        run(range(n))
+    return plan
+
+
+def _best_pole_lines(obj, idx, res):
+    """One line per frequency from the 10 poles' results, as the reference
+    prints it (start_CUDA.cu:1200-1229): NaN-safe, the earliest pole wins ties."""
     lines = np.zeros((len(idx), 6))
     for q in range(len(idx)):
         r = res[q]
         best = -1
-        for p in range(native.N_POLES):   # NaN-safe, earliest pole wins ties
+        for p in range(native.N_POLES):
             if best < 0 or (not np.isnan(r[p, 0]) and not (r[p, 0] >= r[best, 0])):
                 best = p
         b = r[best]
         lines[q] = (24 * b[2], b[0], b[0] * b[0] * obj.n_points, b[1], b[3], b[4])
-    return idx, lines, res
+    return lines
+
+
+def screened_scan(obj, net, conw_r, top=0.034, halo=1, audit=0.02, seed=0, device=0,
+                  precision=native.PRECISION_FP64, margin=AUDIT_MARGIN, pred=None):
+    """Fits the screened frequencies (after the convexity-weight search,
+    whose conw_r is passed in), expanding around a best line at the edge of
+    a fitted run and falling back to the whole grid when the audit sample
+    contradicts the ranking (plan_scan).  Returns (frequency indices
+    1-based, lines, per-fit results [n, 10, 6], Plan)."""
+    if pred is None:
+        pred = net.predict(normalise(features(obj, frequencies(obj), device)))
+    store = {}
+    with native.Engine(obj, device) as eng:
+        eng.set_precision(precision)
+        eng.configure(conw_r=conw_r)
+
+        def fit(idx0):
+            nf = np.repeat(idx0 + 1, native.N_POLES).astype(np.int32)
+            pl = np.tile(np.arange(native.N_POLES), len(idx0)).astype(np.int32)
+            res, _, _ = eng.fit_items(nf, pl)
+            res = res.reshape(len(idx0), native.N_POLES, 6)
+            lines = _best_pole_lines(obj, idx0, res)
+            for i, q in enumerate(idx0.tolist()):
+                store[q] = (res[i], lines[i])
+            return lines[:, 1]
+
+        plan = plan_scan(pred, fit, top, halo, audit, seed, margin)
+    idx = np.array(plan.fitted, dtype=np.int64)
+    res = np.stack([store[i][0] for i in idx])
+    lines = np.stack([store[i][1] for i in idx])
+    return idx + 1, lines, res, plan
 
 
 def best_line(lines):

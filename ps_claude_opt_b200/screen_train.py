@@ -147,15 +147,17 @@ def full_scans(n_obj, seed0=EVAL_SEED, log=print):
     return out
 
 
-def judge(net, fulls, top=0.034, halo=1, audit=0.02, log=print):
+def judge(net, fulls, top=0.034, halo=1, audit=0.02, log=print, precision=native.PRECISION_FP64):
     """Screened scan vs full scan on held-out objects: the screened best line
     must be the full scan's (same frequency, or period within 0.1 h, rms
-    within 0.1 and pole within 1 degree)."""
+    within 0.1 and pole within 1 degree).  Each row also records whether the
+    scan expanded around an edge or fell back to the whole grid."""
     hits, rows = 0, []
     for i, (seed, full, conw_r, t_full) in enumerate(fulls):
         obj, _ = make_object(int(seed))
         t0 = time.time()
-        idx, lines, _ = screen.screened_scan(obj, net, conw_r, top, halo, audit, seed=i)
+        idx, lines, _, plan = screen.screened_scan(obj, net, conw_r, top, halo, audit, seed=i,
+                                                   precision=precision)
         t_scr = time.time() - t0
         bf, bs = screen.best_line(full), screen.best_line(lines)
         fb, sb = full[bf], lines[bs]
@@ -164,7 +166,9 @@ def judge(net, fulls, top=0.034, halo=1, audit=0.02, log=print):
                                      abs(fb[5] - sb[5]) < 1.0)
         hits += ok
         rows.append(dict(seed=int(seed), full_best=int(bf + 1), screened_best=int(idx[bs]), ok=bool(ok),
-                         full_s=float(t_full), screened_s=t_scr, fitted=len(idx), n_freq=len(full)))
+                         full_s=float(t_full), screened_s=t_scr, fitted=len(idx), n_freq=len(full),
+                         initial=plan.initial, expansions=plan.expansions, fallback=plan.fallback,
+                         reason=plan.reason))
         log(json.dumps(rows[-1]))
     return hits, rows
 

@@ -88,3 +88,70 @@ def test_selection_is_deterministic_and_bounded():
     top = np.argsort(pred, kind="stable")[:170]
     assert set(top.tolist()) <= set(a.tolist())
     assert np.all(np.diff(a) > 0)
+
+
+def _landscape(n, best, depth=0.5, base=0.05, seed=0):
+    """Best rms per frequency: noise around `base`, a dip of `depth` at `best`."""
+    rng = np.random.default_rng(seed)
+    r = base * (1.0 + 0.2 * rng.random(n))
+    r[best] = base * depth
+    return r
+
+
+def _plan(pred, rms, **kw):
+    from ps_claude_opt_b200 import screen
+
+    calls = []
+
+    def fit(idx):
+        calls.append(len(idx))
+        return rms[idx]
+
+    return screen.plan_scan(pred, fit, **kw), calls
+
+
+def test_plan_keeps_a_well_screened_scan_small():
+    n = 2000
+    rms = _landscape(n, best=777)
+    pred = np.log(rms)                     # a perfect ranking
+    plan, calls = _plan(pred, rms)
+    assert not plan.fallback and plan.expansions == 0
+    assert plan.best() == 777 and len(plan.fitted) == plan.initial <= 0.122 * n + 1
+    assert len(calls) == 1
+
+
+def test_plan_expands_around_a_best_line_at_a_run_edge():
+    from ps_claude_opt_b200 import screen
+
+    n = 2000
+    rms = _landscape(n, best=1000)
+    rms[1001:1006] = np.linspace(0.024, 0.020, 5)   # the minimum is wide, falling ...
+    rms[1006] = 0.01                                 # ... to its deepest beyond the screened run
+    pred = np.full(n, 5.0)
+    pred[998:1001] = -5.0                             # the network ranks only 998..1000 first
+    plan, _ = _plan(pred, rms, top=0.0015, halo=1, audit=0.0005)
+    assert not plan.fallback and plan.expansions == 3
+    assert plan.best() == 1006 and {1005, 1007} <= set(plan.fitted)
+    assert len(plan.fitted) < 0.05 * n
+
+
+def test_plan_falls_back_when_the_audit_contradicts_the_ranking():
+    n = 2000
+    rms = _landscape(n, best=300)
+    pred = -np.log(rms)                     # an inverted ranking: the screen misses the dip
+    pred[300] = 10.0
+    plan, _ = _plan(pred, np.where(np.arange(n) == 300, 0.025, rms), audit=0.05)
+    # the top-ranked frequencies all sit near base rms; random audit frequencies
+    # reach within 10 % of them, so the scan falls back to the whole grid
+    assert plan.fallback and plan.reason == "audit"
+    assert plan.fitted == list(range(n)) and plan.best() == 300
+
+
+def test_plan_falls_back_after_too_many_expansions():
+    n = 500
+    rms = np.linspace(1.0, 0.5, n)           # monotone: the best keeps moving to the right edge
+    pred = np.zeros(n)
+    pred[:3] = -1.0
+    plan, _ = _plan(pred, rms, top=0.002, halo=0, audit=0.002, max_expansions=3)
+    assert plan.fallback and plan.reason in ("edge", "audit") and len(plan.fitted) == n
+    assert plan.best() == n - 1

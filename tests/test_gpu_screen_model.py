@@ -24,8 +24,11 @@ def test_screen_finds_the_full_scan_best_line_with_a_tenth_of_the_fits():
     for row in rows:
         obj, _ = screen_train.make_object(row["seed"])
         assert obj.grid.n_max == row["n_freq"]
-        idx, lines, _ = screen.screened_scan(obj, net, row["conw_r"])
-        assert len(idx) <= 0.125 * row["n_freq"]
+        idx, lines, _, plan = screen.screened_scan(obj, net, row["conw_r"])
+        if not plan.fallback:
+            assert len(idx) <= 0.13 * row["n_freq"]
+        else:   # the audit sample or an edge sent the scan to the whole grid
+            assert len(idx) == row["n_freq"]
         b = screen.best_line(lines)
         if idx[b] == row["best_freq"]:
             net_hits += 1
@@ -42,7 +45,8 @@ def test_screened_scan_in_mixed_precision_finds_the_same_line():
 
     row = json.load(open(FIXTURE))[0]
     obj, _ = screen_train.make_object(row["seed"])
-    idx, lines, _ = screen.screened_scan(obj, screen.load_model(), row["conw_r"], precision=native.PRECISION_MIXED)
+    idx, lines, _, _ = screen.screened_scan(obj, screen.load_model(), row["conw_r"],
+                                            precision=native.PRECISION_MIXED)
     b = screen.best_line(lines)
     assert idx[b] == row["best_freq"]
     assert abs(lines[b, 0] - row["best_line"][0]) < 1e-4 and abs(lines[b, 1] - row["best_line"][1]) < 1e-4
