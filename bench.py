@@ -43,11 +43,14 @@ METRIC = ("LM fits/s of the plain FP64 full scan of the production object on 1 B
           "the screened+mixed scan in the same line)")
 
 
-def workload():
+def workload(setup_fn=None):
+    """The production object.  setup_fn builds its shape tables: the
+    library's (default) or, for the CPU arms, the oracle's, so that those
+    arms load no product code."""
     from ps_claude_opt_b200 import objects, synth
 
     text, truth = synth.generate(synth.C2, SEED)
-    return objects.parse_input(text), truth
+    return objects.parse_input(text, setup_fn=setup_fn), truth
 
 
 def flops_per_fit(obj, niter):
@@ -138,7 +141,9 @@ def reference_arm(args, rank, world):
     stands in.  Under torchrun rank 0 alone runs it; the others exit."""
     if rank != 0:
         return
-    obj, _ = workload()
+    import oracle
+
+    obj, _ = workload(setup_fn=oracle.setup_shape)
     cores = os.cpu_count() or 1
     per_step = max(8, cores)
     freq_at = lambda s: 1 + s * (per_step // 10 + 1)  # noqa: E731

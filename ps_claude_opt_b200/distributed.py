@@ -5,8 +5,11 @@ frequencies (start_CUDA.cu:792-1245) share nothing but the object -- so the
 scan shards without a data-path collective.  Each rank takes whole
 frequencies (all 10 poles of a frequency on one rank, so the best-pole choice
 of start_CUDA.cu:1200-1229 stays local) in contiguous blocks dealt
-round-robin, fits them through its own engine, and only the finished lines
-travel: one gather of (first frequency, lines) pairs to rank 0.
+round-robin -- by default eight blocks per rank, so frequencies whose fits
+converge early or late (stop condition < 1 makes iteration counts ragged)
+spread over all ranks instead of piling onto one -- fits them through its own
+engine, and only the finished lines travel: one gather of (first frequency,
+lines) pairs to rank 0.
 
 The convexity-weight search (CUDAPrecalc, start_CUDA.cu:400-789) runs on rank
 0 and its conw_r is broadcast, so every rank scans with the same weight.
@@ -32,15 +35,19 @@ class ScanError(RuntimeError):
             sorted(self.failures), "; ".join(f"{r}: {m}" for r, m in sorted(self.failures.items()))))
 
 
+BLOCKS_PER_RANK = 8
+
+
 def frequency_blocks(n_start: int, n_last: int, world: int, rank: int, block: int | None = None):
     """Blocks (first frequency, count) of frequencies n_start..n_last that
     `rank` of `world` fits.  Blocks of `block` frequencies go round-robin;
-    the default, one block per rank, gives each rank one contiguous range."""
+    the default interleaves BLOCKS_PER_RANK blocks per rank (one block when
+    there is one rank)."""
     total = max(0, n_last - n_start + 1)
     if total == 0:
         return []
     if block is None:
-        block = -(-total // world)
+        block = total if world == 1 else -(-total // (world * BLOCKS_PER_RANK))
     if block < 1:
         raise ValueError("block must be >= 1")
     out = []

@@ -123,7 +123,11 @@ def test_frequency_blocks_cover_each_frequency_once():
                 seen.extend(range(lo, lo + cnt))
         assert sorted(seen) == list(range(n_start, n_last + 1))
     assert frequency_blocks(5, 4, 2, 0) == []
-    assert frequency_blocks(1, 10, 2, 0) == [(1, 5)] and frequency_blocks(1, 10, 2, 1) == [(6, 5)]
+    # default: BLOCKS_PER_RANK interleaved blocks per rank; one block on one rank
+    assert frequency_blocks(1, 10, 1, 0) == [(1, 10)]
+    assert frequency_blocks(1, 10, 2, 0) == [(1, 1), (3, 1), (5, 1), (7, 1), (9, 1)]
+    assert frequency_blocks(1, 5000, 8, 3) == [(lo, 79) for lo in range(1 + 3 * 79, 5001, 8 * 79)][:8]
+    assert sum(c for r in range(8) for _, c in frequency_blocks(1, 5000, 8, r)) == 5000
 
 
 @pytest.mark.parametrize("block", [None, 1, 4])
