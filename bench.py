@@ -53,6 +53,230 @@ def workload(setup_fn=None):
     return objects.parse_input(text, setup_fn=setup_fn), truth
 
 
+def _c3_text(i):
+    from ps_claude_opt_b200 import synth
+
+    cfg, seed = synth.config3_object(i)
+    return synth.generate(cfg, seed)[0]
+
+
+def batch_texts(n_obj):
+    """Input texts of the batched workload's objects, generated on host
+    cores by a spawn pool (started before this process touches a GPU)."""
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        return pool.map(_c3_text, range(n_obj))
+
+
+def bench_batch(texts, max_freq, device=0):
+    """The batched form on the config-3 objects: the convexity-weight search
+    and the first `max_freq` frequencies of every object's scan, all objects
+    in one ps_gpu_scan_batch call (one persistent launch per coefficient
+    group, scans captured in one CUDA graph), with the autotuned tile
+    layouts, with the first layout that fits, and object by object
+    (run_object).  Wall times; the lines must agree bit for bit."""
+    from ps_claude_opt_b200 import native, objects
+
+    t0 = time.perf_counter()
+    objs = [objects.parse_input(t) for t in texts]
+    t_setup = time.perf_counter() - t0
+    out = {}
+    native.batch_set_tuning(1)
+    t0 = time.perf_counter()
+    tuned_first = native.scan_batch(objs, device=device, max_freq=max_freq)
+    out["tuned_first_call_s"] = time.perf_counter() - t0   # includes timing the candidate layouts
+    report = native.batch_tuning_report()
+    t0 = time.perf_counter()
+    tuned = native.scan_batch(objs, device=device, max_freq=max_freq)
+    out["tuned_s"] = time.perf_counter() - t0               # layouts from the cache
+    native.batch_set_tuning(0)
+    t0 = time.perf_counter()
+    first_fit = native.scan_batch(objs, device=device, max_freq=max_freq)
+    out["first_fit_s"] = time.perf_counter() - t0
+    native.batch_set_tuning(1)
+    t0 = time.perf_counter()
+    one = [native.run_object(o, device=device, max_freq=max_freq) for o in objs]
+    out["one_by_one_s"] = time.perf_counter() - t0
+    same = all(np.array_equal(a[0], b[0]) and np.array_equal(a[0], c[0]) and np.array_equal(a[0], d[0]) and
+               a[1] == b[1] == c[1] == d[1] for a, b, c, d in zip(tuned, tuned_first, first_fit, one))
+    # fits: 100 per convexity-weight round (10 test periods x 10 poles; the
+    # weight doubles each round after the first) plus the scan's
+    fits = 0
+    for o, (lines, cw) in zip(objs, tuned):
+        rounds = int(round(np.log2(cw / o.conw_r))) + 1
+        fits += 100 * rounds + 10 * len(lines)
+    pts = [o.n_points for o in objs]
+    out.update({
+        "objects": len(objs), "fits": fits, "fits_per_s": fits / out["tuned_s"],
+        "s_per_object": out["tuned_s"] / len(objs), "host_setup_s": t_setup,
+        "tuned_vs_first_fit": out["first_fit_s"] / out["tuned_s"],
+        "batch_vs_one_by_one": out["one_by_one_s"] / out["tuned_s"],
+        "lines_identical_across_forms": bool(same), "tuning": report,
+        "workload": "config 3: %d objects, %d-%d points, lmax %s, %d-%d facets, first %d frequencies of each "
+                    "scan after the convexity-weight search, stop condition 0.005 (ragged iterations), FP64" % (
+                        len(objs), min(pts), max(pts), sorted({o.l_max for o in objs}),
+                        min(o.n_fac for o in objs), max(o.n_fac for o in objs), max_freq),
+    })
+    return out
+
+
+def run_program(cmd, text, timeout=1200):
+    """Runs a period_search-style program in a fresh directory on
+    period_search_in = text; returns (rc, wall seconds, output lines)."""
+    import shutil
+
+    d = tempfile.mkdtemp(prefix="psbench_")
+    try:
+        with open(os.path.join(d, "period_search_in"), "w") as f:
+            f.write(text)
+        t0 = time.perf_counter()
+        r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=timeout)
+        wall = time.perf_counter() - t0
+        p = os.path.join(d, "period_search_out")
+        lines = [l for l in open(p).read().splitlines() if l.strip()] if os.path.exists(p) else []
+        return r.returncode, wall, lines
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def program_scan_rate(cmd, name):
+    """Scan fits/s of a period_search-style program on REFERENCE_INPUTS[name]:
+    (lines - 1) x 10 fits / (wall time of the whole input - wall time of its
+    one-frequency copy), which takes start-up, tables and the
+    convexity-weight search out of both."""
+    from ps_claude_opt_b200 import synth
+
+    rc1, w1, _ = run_program(cmd, synth.reference_input_text(name, one_freq=True))
+    rc, w, lines = run_program(cmd, synth.reference_input_text(name))
+    ok = rc == 0 and rc1 == 0 and len(lines) > 1 and w > w1
+    fits = 10 * (len(lines) - 1)
+    return {"rc": rc, "wall_s": w, "wall_one_freq_s": w1, "lines": len(lines),
+            "scan_fits_per_s": fits / (w - w1) if ok else None,
+            "s_per_object_scan": (w - w1) if ok else None}, lines
+
+
+def reference_gpu_leg(names=("c1", "c2rel")):
+    """The reference's own GPU application (unchanged, sm_100a build) and
+    this project's host program on the same inputs and the same B200, timed
+    the same way (program_scan_rate), with the comparator's verdict of our
+    lines against the reference's."""
+    from ps_claude_opt_b200 import compare, native
+
+    app = os.path.join(ROOT, "oracle", "_ref", "refapp_sm100a")
+    if not os.path.exists(app):
+        return {"unavailable": "oracle/_ref/refapp_sm100a not built (oracle/refapp/build.sh)"}
+    out = {}
+    for name in names:
+        ref, ref_lines = program_scan_rate([app, "--device", "0"], name)
+        ours, our_lines = program_scan_rate([native.HOST_PROGRAM, "--fresh"], name)
+        c = compare.compare_lines(our_lines, ref_lines)
+        out[name] = {"reference_app": ref, "ours_host_program": ours,
+                     "speedup_scan": (ours["scan_fits_per_s"] / ref["scan_fits_per_s"])
+                     if ours["scan_fits_per_s"] and ref["scan_fits_per_s"] else None,
+                     "speedup_whole_program": ref["wall_s"] / ours["wall_s"] if ours["wall_s"] else None,
+                     "lines_vs_reference": {"pole_or_dark_mismatches": c.pole_mismatch, "worst": list(c.worst),
+                                            "outside_envelope": c.envelope_violations,
+                                            "best_line_same": c.best_line_same, "identical": c.identical,
+                                            "n_lines": c.n_lines}}
+    return out
+
+
+def c1_leg(steps, warmup, device, cpu=True):
+    """Config 1 (lmax 3, 288 facets, 1200 relative points): the whole
+    object's scan, 200 frequencies x 10 poles = 2000 fits, as ONE launch,
+    device-timed with CUDA events (the convexity-weight search left out);
+    and the oracle on all host cores on a bounded sample of the same fits."""
+    import torch
+
+    from ps_claude_opt_b200 import native, objects, synth
+
+    text, _ = synth.generate(synth.C1, 1000003)
+    obj = objects.parse_input(text)
+    n = obj.grid.n_max * 10
+    items = np.zeros((n, 2), dtype=np.int32)
+    items[:, 0] = 1 + np.arange(n) // 10
+    items[:, 1] = np.arange(n) % 10
+    eng = native.Engine(obj, device=device)
+    eng.configure(conw_r=obj.conw_r)
+    stream = torch.cuda.ExternalStream(eng.stream)
+    d_items = torch.from_numpy(items).cuda()
+    d_out = torch.empty(n * ctypes.sizeof(native.FitResult), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    ms = []
+    with torch.cuda.stream(stream):
+        for s in range(warmup + steps):
+            flush.fill_(s & 0xFF)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.fit_items_device(n, d_items.data_ptr(), d_out.data_ptr())
+            e1.record(stream)
+            if s >= warmup:
+                ms.append((e0, e1))
+    torch.cuda.synchronize()
+    t = [a.elapsed_time(b) for a, b in ms]
+    eng.close()
+    value = n / (np.mean(t) / 1000.0)
+    out = {"value": value, "unit": "fits/s", "s_per_object": n / value, "fits_per_launch": n, "steps": steps,
+           "ms_per_step": float(np.mean(t)), "gpu_launches": steps,
+           "workload": "config 1 object 0: lmax 3 (16 coeffs), 288 facets, 1200 relative points, "
+                       "200 frequencies x 10 poles, 50 LM iterations, FP64, one launch per step"}
+    if cpu:
+        import oracle
+
+        cobj = objects.parse_input(text, setup_fn=oracle.setup_shape)
+        cores = os.cpu_count() or 1
+        nc = 4 * cores
+        om = oracle.OracleModel(cobj)
+        t0 = time.perf_counter()
+        om.fit_batch(cobj.grid.freq_start, cobj.grid.freq_step, items[:nc, 0], items[:nc, 1], threads=cores,
+                     fast=True)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": nc / dt, "unit": "fits/s", "cores": cores, "kind": "port",
+                               "s_per_object": n / (nc / dt),
+                               "sample": "%d fits (frequencies 1..%d, 10 poles) of the same object, %.1f s" %
+                                         (nc, nc // 10, dt)}
+    return out
+
+
+def _best_pole_lines(res, n_points):
+    """One line per frequency (10 consecutive poles) as the reference prints
+    it: NaN-safe best rms, the earliest pole wins ties (start_CUDA.cu:1200-1229)."""
+    lines = []
+    for q in range(len(res) // 10):
+        r = res[10 * q:10 * q + 10]
+        b = -1
+        for p in range(10):
+            if b < 0 or (not np.isnan(r["dev"][p]) and not (r["dev"][p] >= r["dev"][b])):
+                b = p
+        x = r[b]
+        lines.append((24 * x["per"], x["dev"], x["dev"] ** 2 * n_points, x["dark"], x["la"], x["be"]))
+    return np.array(lines)
+
+
+def result_errors(test, ref, n_points):
+    """Differences of two runs of the same (frequency, pole) items: per fit
+    the worst |dP| [h], |d lambda| [deg], |d beta|, |d rms|, |d chi^2| and
+    how many fits print a different pole; per line (best of each frequency's
+    10 poles) the reference's comparator rules."""
+    from ps_claude_opt_b200 import compare, native
+
+    dl = np.abs((test["la"] - ref["la"] + 180.0) % 360.0 - 180.0)
+    printed = (np.round(test["la"]) != np.round(ref["la"])) | (np.round(test["be"]) != np.round(ref["be"]))
+    lt = native.format_lines(_best_pole_lines(test, n_points)).splitlines()
+    lr = native.format_lines(_best_pole_lines(ref, n_points)).splitlines()
+    c = compare.compare_lines(lt, lr)
+    return {"fits": int(len(test)),
+            "max_abs": {"period_h": float(np.max(np.abs(test["per"] - ref["per"])) * 24),
+                        "lambda_deg": float(np.max(dl)), "beta_deg": float(np.max(np.abs(test["be"] - ref["be"]))),
+                        "rms": float(np.max(np.abs(test["dev"] - ref["dev"]))),
+                        "chi2": float(np.max(np.abs(test["chisq"] - ref["chisq"])))},
+            "fits_printed_pole_differs": int(np.sum(printed)),
+            "fits_pole_off_gt1deg": int(np.sum((dl > 1.0) | (np.abs(test["be"] - ref["be"]) > 1.0))),
+            "lines": int(len(lt)), "lines_pole_or_dark_mismatch": c.pole_mismatch,
+            "lines_outside_envelope": c.envelope_violations, "best_line_same": c.best_line_same}
+
+
 def flops_per_fit(obj, niter):
     """Algorithmic FLOPs of one fit: (niter + 1) evaluations + niter solves,
     per-point cost F_pt = 150 + 10 Nf + V (60 + 2 nc) + mfit (mfit + 1) +
@@ -193,6 +417,11 @@ def profile_case(mixed=False):
               (n, niter.mean(), flops_per_fit(obj, niter.mean()) * n))
 
 
+RESULT_DTYPE = np.dtype([("dev", "f8"), ("dark", "f8"), ("per", "f8"), ("la", "f8"), ("be", "f8"),
+                         ("chisq", "f8"), ("niter", "i4"), ("status", "i4")])
+FIXTURE = os.path.join(ROOT, "tests", "golden", "bench_object_fullscan.json")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -201,6 +430,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--fits-per-cta", type=int, default=FITS_PER_CTA)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="only the headline legs (FP64 timed steps, end to end, mixed); skip config 1, the "
+                         "reference GPU app, the screened scan and the batch")
+    ap.add_argument("--batch-objects", type=int, default=None)
+    ap.add_argument("--batch-freqs", type=int, default=4)
     ap.add_argument("--profile-case", action="store_true",
                     help="two fit-kernel launches (warm-up + one to capture), one fit per resident CTA")
     ap.add_argument("--mixed", action="store_true", help="with --profile-case: the mixed-precision kernel")
@@ -215,6 +449,13 @@ def main():
     if args.profile_case:
         profile_case(args.mixed)
         return
+
+    from ps_claude_opt_b200 import synth
+
+    extra = rank == 0 and world == 1 and not args.no_extra
+    # host-side generation of the batched workload, before this process touches a GPU
+    n_batch = synth.C3_OBJECTS if args.batch_objects is None else args.batch_objects
+    batch_in = batch_texts(n_batch) if extra and n_batch > 0 else None
 
     import torch
 
@@ -250,12 +491,27 @@ def main():
     stream = torch.cuda.ExternalStream(eng.stream)
     d_items = [torch.from_numpy(items_for(s)).cuda() for s in range(steps_total)]
     rec = ctypes.sizeof(native.FitResult)   # one ps_fit_result per fit
+    assert RESULT_DTYPE.itemsize == rec
     d_out = torch.empty(n_fits * rec, dtype=torch.uint8, device="cuda")
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     torch.cuda.synchronize()
 
     def run_step(s):
         eng.fit_items_device(n_fits, d_items[s].data_ptr(), d_out.data_ptr())
+
+    def timed_steps():
+        evs = []
+        with torch.cuda.stream(stream):
+            for s in range(args.warmup, steps_total):
+                flush.fill_(s & 0xFF)   # L2 flush between timed launches (not timed)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                run_step(s)
+                e1.record(stream)
+                evs.append((e0, e1))
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
 
     with torch.cuda.stream(stream):
         for s in range(args.warmup):
@@ -268,29 +524,15 @@ def main():
 
     clocks = ClockSampler(local_rank)
     clocks.start()
-    evs = []
-    with torch.cuda.stream(stream):
-        for s in range(args.warmup, steps_total):
-            flush.fill_(s & 0xFF)   # L2 flush between timed launches (not timed)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            run_step(s)
-            e1.record(stream)
-            evs.append((e0, e1))
-    torch.cuda.synchronize()
-    ms = [a.elapsed_time(b) for a, b in evs]
+    ms = timed_steps()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     clk = clocks.stop()
     total_ms = float(sum(ms))
 
-    # read back the last step: iteration counts for the FLOP count, and a sanity check
-    res = np.frombuffer(d_out.cpu().numpy().tobytes(), dtype=np.dtype(
-        [("dev", "f8"), ("dark", "f8"), ("per", "f8"), ("la", "f8"), ("be", "f8"), ("chisq", "f8"),
-         ("niter", "i4"), ("status", "i4")]))
-    assert res.dtype.itemsize == rec
+    # the last step's results: iteration counts for the FLOP count, a sanity check
+    res = np.frombuffer(d_out.cpu().numpy().tobytes(), dtype=RESULT_DTYPE).copy()
     niter = float(np.mean(res["niter"]))
     if not np.all(np.isfinite(res["per"])):
         raise RuntimeError("non-finite fit results")
@@ -327,38 +569,14 @@ def main():
         flush.fill_(1)
         run_step(0)
     torch.cuda.synchronize()
-    evm = []
-    with torch.cuda.stream(stream):
-        for s in range(args.warmup, steps_total):
-            flush.fill_(s & 0xFF)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            run_step(s)
-            e1.record(stream)
-            evm.append((e0, e1))
-    torch.cuda.synchronize()
-    mixed_ms = float(sum(a.elapsed_time(b) for a, b in evm))
+    mixed_ms = float(sum(timed_steps()))
+    res_m = np.frombuffer(d_out.cpu().numpy().tobytes(), dtype=RESULT_DTYPE).copy()
     if dist:
         t = torch.tensor([mixed_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         mixed_ms = float(t.item())
     mixed_value = n_fits * args.steps * world / (mixed_ms / 1000.0)
-
-    # the screened + mixed scan of the whole object, end to end on this GPU:
-    # features of all trial frequencies, the network's ranking, the mixed
-    # fits of the chosen frequencies (all 10 poles) -- the convexity-weight
-    # search, the same for both kinds of scan, is left out of both
-    from ps_claude_opt_b200 import screen
-
-    net = screen.load_model()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    pred = net.predict(screen.normalise(screen.features(obj, screen.frequencies(obj), local_rank)))
-    sel = screen.select(pred) + 1
-    t_rank = time.perf_counter() - t0
-    eng.fit_items(np.repeat(sel, 10), np.tile(np.arange(10), len(sel)))
-    screened_s = time.perf_counter() - t0
+    eng.close()
 
     line = None
     if rank == 0:
@@ -388,16 +606,13 @@ def main():
             "e2e": {"value": e2e_value, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": float(np.mean(e2e_ms))},
             "gpu_launches": args.steps,
-            "screened_mixed": {"s_per_object": screened_s, "ranking_s": t_rank, "fitted_frequencies": int(len(sel)),
-                               "n_frequencies": int(n_max), "fits": int(10 * len(sel)),
-                               "vs_plain_fp64_full_scan_s": n_obj / (value / world),
-                               "note": "top 3.4 % of the network's ranking with one neighbour each side plus a "
-                                       "2 % random audit; mixed-precision fits; trained network from "
-                                       "ps_claude_opt_b200/screen_model.bin"},
             "mixed": {"value": mixed_value, "unit": "fits/s", "ms_per_step": mixed_ms / args.steps,
                       "s_per_object": n_obj / (mixed_value / world), "gpu_launches": args.steps,
-                      "precision": "facet sweep FP32 with 3xTF32 tensor-core shape derivatives; geometry, "
-                                   "J^T W J, chi^2, Gauss-Jordan and lambda update FP64"},
+                      "speedup_vs_fp64": mixed_value / value,
+                      "precision": "facet sweep FP32 (Newton-refined reciprocal, per-point sums flushed to FP64 "
+                                   "every 8 facets) with 3xTF32 tensor-core shape derivatives; geometry, "
+                                   "J^T W J, chi^2, Gauss-Jordan and lambda update FP64",
+                      "errors_vs_fp64": result_errors(res_m, res, obj.n_points)},
         }
         if world == 1 and not args.no_cpu_baseline:
             cores = os.cpu_count() or 1
@@ -406,8 +621,50 @@ def main():
             line["cpu_baseline"] = {"value": rate, "unit": "fits/s", "cores": cores, "kind": "port",
                                     "sample": "%d fits (frequencies 1.., 10 poles) of the same object, %.1f s" %
                                               (n_cpu, dt)}
+    if extra:
+        from ps_claude_opt_b200 import screen
+
+        # the screened + mixed scan of the whole object, end to end on this
+        # GPU: features of all trial frequencies, the network's ranking, the
+        # mixed fits of the chosen frequencies (all 10 poles), widening at run
+        # edges and the audit's fallback.  The convexity-weight search, the
+        # same for both kinds of scan, is left out of both: the scan uses the
+        # weight the full FP64 scan of the fixture ended with.
+        fix = json.load(open(FIXTURE)) if os.path.exists(FIXTURE) else None
+        conw_r = fix["conw_r"] if fix else obj.conw_r
+        net = screen.load_model()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pred = net.predict(screen.normalise(screen.features(obj, screen.frequencies(obj), local_rank)))
+        t_rank = time.perf_counter() - t0
+        idx, lines, _, plan = screen.screened_scan(obj, net, conw_r, device=local_rank,
+                                                   precision=native.PRECISION_MIXED, pred=pred)
+        screened_s = time.perf_counter() - t0
+        b = screen.best_line(lines)
+        sm = {"s_per_object": screened_s, "ranking_s": t_rank, "fitted_frequencies": int(len(idx)),
+              "first_selection": plan.initial, "edge_expansions": plan.expansions, "fallback": plan.fallback,
+              "fallback_reason": plan.reason, "n_frequencies": int(n_max), "fits": int(10 * len(idx)),
+              "vs_plain_fp64_full_scan_s": n_max * 10 / value,
+              "speedup_vs_plain_fp64_full_scan": (n_max * 10 / value) / screened_s,
+              "best_frequency": int(idx[b]),
+              "note": "top 3.4 % of the network's ranking with one neighbour each side plus a 2 % random audit, "
+                      "widened around a best line at a run edge, full grid if the audit contradicts the ranking; "
+                      "mixed-precision fits; trained network ps_claude_opt_b200/screen_model.bin"}
+        if fix:
+            got = native.format_lines(lines[b:b + 1]).strip()
+            sm["best_line_matches_full"] = bool(int(idx[b]) == fix["best_freq"] and
+                                                got.split()[3:] == fix["formatted_best"].split()[3:] and
+                                                abs(lines[b, 0] - fix["best_line"][0]) < 0.1 and
+                                                abs(lines[b, 1] - fix["best_line"][1]) < 0.1)
+            sm["best_line"] = got
+            sm["full_scan_best_line"] = fix["formatted_best"]
+        line["screened_mixed"] = sm
+        line["c1"] = c1_leg(args.steps, args.warmup, local_rank, cpu=not args.no_cpu_baseline)
+        line["reference_gpu"] = reference_gpu_leg()
+        if batch_in:
+            line["batch"] = bench_batch(batch_in, args.batch_freqs, device=local_rank)
+    if rank == 0:
         print(json.dumps(line), flush=True)
-    eng.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

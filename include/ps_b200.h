@@ -160,6 +160,21 @@ ps_status ps_gpu_scan_batch(int32_t device, int32_t n_obj, const ps_object *objs
                             ps_line *lines, const int64_t *line_offset, int32_t *n_lines,
                             double *conw_r_out);
 
+/* Tile layout of ps_gpu_scan_batch's groups (no reference counterpart):
+   mode 1 (default) times every layout that fits in shared memory -- 32 or 16
+   rows per J^T W J tile, per-curve statistics in shared memory or in the
+   scratch slab -- on a one-wave, three-iteration sample of the group's own
+   items and keeps the fastest (cached per group shape for the process;
+   setting mode 1 clears the cache); mode 0 takes the first layout that fits
+   in that order.  Results do not depend on the layout. */
+ps_status ps_batch_set_tuning(int32_t mode);
+/* JSON description of the last ps_gpu_scan_batch's groups: padded
+   coefficient count, objects, resident CTAs, candidate layouts with their
+   sample times (ms; -1 where not timed), the chosen layout and whether it
+   was timed, cached or the only one.  Copies at most len - 1 bytes and a
+   terminating NUL into buf; returns the full length. */
+int32_t ps_batch_tuning_report(char *buf, int32_t len);
+
 /* ---- finer-grained entry points (no reference counterpart: the reference
         keeps these steps inside CUDAStart) ---- */
 
@@ -198,7 +213,8 @@ ps_status ps_gpu_set_quirks(ps_gpu *h, int32_t quirks);
    facet sweep -- brightness, its parameter derivatives and the per-point
    sums -- runs in FP32, its shape-derivative products on the tensor cores
    as 3xTF32 (high x high + high x low + low x high) with FP32 accumulation,
-   the per-point scalar sums flushed to FP64 every 32 facets; geometry,
+   the reciprocal of each facet term Newton-refined and the per-point scalar
+   sums flushed to FP64 every 8 facets; geometry,
    J^T W J, chi^2, the Gauss-Jordan solve and the lambda update stay FP64.
    For n_coef <= 64 (lmax <= 7).  Takes effect at the next configure (or
    precalc / start, which configure). */
@@ -226,10 +242,15 @@ ps_status ps_gpu_occupancy(ps_gpu *h, int32_t *ctas_per_sm, int32_t *n_sm);
    arguments of ps_gpu_prepare + ps_gpu_configure + ps_gpu_fit_items as host
    arrays and writes host results; allocates nothing, on the device or the
    host heap.  All device data live in one file-scope 64 MiB __device__
-   array, present on every GPU that loads the library until the process
-   exits.  The first call on a device looks up that array's address with the
-   device current and sets the kernel's shared-memory limit: make it before
-   any stream capture.  Calls share the array and leave their data in it;
+   array per GPU.  CUDA loads modules lazily, so the array is reserved when
+   the first call on a device loads the library's module there, and is held
+   until the process exits; a call with n = 0 (every other argument may be
+   NULL) does only that -- select the device, load the module, look up the
+   array -- so a caller can reserve the 64 MiB at start-up, before its own
+   allocator fills the device.  Each call looks up the array's device address
+   with the device current; the first call with work also sets the kernel's
+   shared-memory limit: make it before any stream capture.  Calls share the
+   array and leave their data in it;
    calls that overlap on the GPU race -- serialise them.  Objects whose tables
    plus one CTA's scratch exceed 64 MiB, or with more than 200 lightcurves,
    are rejected with PS_ERR_ARG; smaller ones run on as many CTAs as the

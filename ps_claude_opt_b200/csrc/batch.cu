@@ -14,11 +14,30 @@
 // items of the objects still searching; the scan launches of all groups are
 // captured into one CUDA graph (a fork over the groups' streams and a join)
 // and replayed.  The groups' launches run concurrently on their streams.
+//
+// Two scheduling choices are made per group:
+//  * the tile layout (rows per J^T W J tile: 32, which allows the k-slice
+//    mode, or 16; per-curve statistics in shared memory or in the scratch
+//    slab) is picked by a small autotuner: every layout that fits in shared
+//    memory is timed on a one-wave sample of the group's own items cut to
+//    three LM iterations, and the fastest is kept for the group's shape
+//    (cached per process); ps_batch_set_tuning(0) takes the first layout that
+//    fits instead;
+//  * items go into the queue largest object first (longest-processing-time
+//    order by an estimate of the per-fit cost), so the most expensive fits
+//    start early and the launch's tail is made of short ones.
+// Neither choice changes a result: every fit runs the same arithmetic.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstring>
 #include <map>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <tuple>
 #include <vector>
 
 #include "engine.h"
@@ -29,10 +48,28 @@
 namespace {
 
 constexpr int kTestPeriods = 10;  // start_CUDA.cu:420
+constexpr int kTuneIterations = 3; // LM iterations of a tuning sample fit
+
+// Tile layouts in order of preference: {rows per J^T W J tile, per-curve
+// statistics in shared memory}.
+constexpr int kLayouts[4][2] = {{32, 1}, {32, 0}, {16, 1}, {16, 0}};
+
+struct Tuning {
+    std::mutex mu;
+    int mode = 1;                                            // 1 autotune, 0 first layout that fits
+    std::map<std::tuple<int, int, int, int, int>, int> cache;  // group shape -> layout index
+    std::string report = "[]";                               // JSON of the last ps_gpu_scan_batch
+};
+Tuning &tuning()
+{
+    static Tuning t;
+    return t;
+}
 
 struct Group {
     int ncp = 0;
     std::vector<int> members;          // object indices
+    std::vector<int> order;            // member positions, most expensive object first
     psb::DevObject env{};              // largest sizes: the shared-memory layout
     size_t per_cta = 0;                // scratch doubles of one CTA (largest object)
     int ctas = 0;                      // resident CTAs of the batch kernel
@@ -84,9 +121,83 @@ int scan_lines(const ps_object &o)
     return std::max(0, std::min(n_max - o.n_start_from + 1, (int)o.max_lines));
 }
 
-// Shared-memory layout of a group: the largest sizes of its objects, the
-// preferred tile layout that fits (beside the kernel's static object copy).
-ps_status plan_group(Batch &b, Group &g, size_t smem_limit)
+// Estimated FP64 work of one LM evaluation of an object (the facet sweep,
+// the J^T W J update and the pseudo-points): the key of the queue order.
+double eval_cost(const psb::DevObject &o)
+{
+    const double nf = o.n_fac, nc = o.n_coef, mf = o.mfit;
+    return o.n_points * (10.0 * nf + 0.45 * nf * (60.0 + 2.0 * nc) + mf * (mf + 1.0)) + 8.0 * nf * nc;
+}
+
+// The group's objects (their current constants) to the device.  iter_cap > 0
+// cuts every fit to that many LM iterations (tuning samples).
+ps_status upload_objects(Batch &b, Group &g, int iter_cap = 0)
+{
+    std::vector<psb::DevObject> objs;
+    std::vector<psb::DevParams> prms;
+    for (int i : g.members) {
+        psb::DevObject o = b.h[i]->obj;
+        o.tile_rows = g.env.tile_rows;
+        o.cstat_smem = g.env.cstat_smem;
+        objs.push_back(o);
+        psb::DevParams p = b.h[i]->prm;
+        p.phase_cycles = nullptr;
+        if (iter_cap > 0) {
+            p.n_iter_max = iter_cap;
+            p.iter_diff_max = 0;
+            p.n_iter_min = 0;
+        }
+        prms.push_back(p);
+    }
+    PSB_CUDA(psb::upload(g.objs, objs, g.stream));
+    PSB_CUDA(psb::upload(g.prms, prms, g.stream));
+    return PS_OK;
+}
+
+// Device time of one launch of the tuning sample (one wave of the group's
+// first items, round-robin over its objects, kTuneIterations iterations
+// each) under the layout now in g.env.
+ps_status time_layout(Batch &b, Group &g, float *ms)
+{
+    PSB_CUDA(cudaStreamSynchronize(g.stream));
+    ps_status st = upload_objects(b, g, kTuneIterations);
+    if (st != PS_OK) return st;
+    std::vector<psb::FitItem> sample;
+    for (int q = 0; (int)sample.size() < g.ctas && q < 64 * PS_N_POLES; ++q)
+        for (size_t k = 0; k < g.members.size() && (int)sample.size() < g.ctas; ++k)
+            sample.push_back(psb::FitItem{1 + q / PS_N_POLES, (q % PS_N_POLES) | (int)k << 8});
+    PSB_CUDA(psb::upload(g.items, sample, g.stream));
+    PSB_CUDA(g.out.ensure(sample.size()));
+    PSB_CUDA(g.scratch.ensure(g.per_cta * sample.size()));
+    PSB_CUDA(g.queue.ensure(1));
+    PSB_CUDA(g.status.ensure(1));
+    PSB_CUDA(cudaMemsetAsync(g.status.ptr, 0, sizeof(int), g.stream));
+    PSB_CUDA(cudaMemsetAsync(g.queue.ptr, 0, sizeof(int), g.stream));
+    const int e = psb::prepare_batch_kernel(g.env);
+    if (e) return psb_fail_cuda(e, "ps_gpu_scan_batch: kernel attributes");
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    PSB_CUDA(cudaEventCreate(&t0));
+    PSB_CUDA(cudaEventCreate(&t1));
+    cudaError_t ce = cudaEventRecord(t0, g.stream);
+    int le = 0;
+    if (ce == cudaSuccess)
+        le = psb::launch_fits_batch(g.env, g.objs.ptr, g.prms.ptr, g.items.ptr, (int)sample.size(), g.queue.ptr,
+                                    g.out.ptr, g.scratch.ptr, g.per_cta, (int)sample.size(), g.status.ptr, g.stream);
+    if (ce == cudaSuccess && !le) ce = cudaEventRecord(t1, g.stream);
+    if (ce == cudaSuccess && !le) ce = cudaEventSynchronize(t1);
+    if (ce == cudaSuccess && !le) ce = cudaEventElapsedTime(ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (le) return psb_fail_cuda(le, "ps_gpu_scan_batch: tuning launch");
+    if (ce != cudaSuccess) return psb_fail_cuda(ce, "ps_gpu_scan_batch: tuning timing");
+    return PS_OK;
+}
+
+// Shared-memory layout of a group: the largest sizes of its objects and a
+// tile layout that fits (beside the kernel's static object copy) -- the
+// autotuner's pick, or the first that fits.  Appends the group's entry to
+// the JSON report.
+ps_status plan_group(Batch &b, Group &g, size_t smem_limit, std::string &report)
 {
     psb::DevObject &e = g.env;
     e = b.h[g.members[0]]->obj;
@@ -98,47 +209,83 @@ ps_status plan_group(Batch &b, Group &g, size_t smem_limit)
         e.row_stride = std::max(e.row_stride, o.row_stride);
         e.ma = std::max(e.ma, o.ma);
     }
-    const int layouts[3][2] = {{32, 1}, {32, 0}, {16, 0}};
-    bool ok = false;
-    for (const auto &l : layouts) {
-        e.tile_rows = l[0];
-        e.cstat_smem = l[1];
-        if (psb::fit_smem_bytes(e.n_fac, e.mfit, e.ncp, e.n_curves, e.row_stride, e.tile_rows, e.cstat_smem, 0) +
-                1024 <= smem_limit) {
-            ok = true;
-            break;
+    std::vector<int> fits;
+    for (int l = 0; l < 4; ++l)
+        if (psb::fit_smem_bytes(e.n_fac, e.mfit, e.ncp, e.n_curves, e.row_stride, kLayouts[l][0], kLayouts[l][1], 0) +
+                1024 <= smem_limit)
+            fits.push_back(l);
+    if (fits.empty()) return psb_fail(PS_ERR_ARG, "ps_gpu_scan_batch: objects too large for shared memory");
+    g.per_cta = 0;
+    for (int i : g.members) g.per_cta = std::max(g.per_cta, psb::fit_scratch_doubles(b.h[i]->obj));
+    // queue order: most expensive object first, ties by position
+    g.order.resize(g.members.size());
+    std::iota(g.order.begin(), g.order.end(), 0);
+    std::stable_sort(g.order.begin(), g.order.end(), [&](int x, int y) {
+        return eval_cost(b.h[g.members[x]]->obj) > eval_cost(b.h[g.members[y]]->obj);
+    });
+
+    auto set_layout = [&](int l) -> ps_status {
+        e.tile_rows = kLayouts[l][0];
+        e.cstat_smem = kLayouts[l][1];
+        const int per_sm = psb::fit_batch_ctas_per_sm(e);
+        if (per_sm < 1) return psb_fail(PS_ERR_CUDA, "ps_gpu_scan_batch: batch kernel cannot be resident");
+        g.ctas = per_sm * b.h[g.members[0]]->n_sm;
+        return PS_OK;
+    };
+    Tuning &t = tuning();
+    int mode;
+    {
+        std::lock_guard<std::mutex> lk(t.mu);
+        mode = t.mode;
+    }
+    const auto key = std::make_tuple(e.ncp, e.n_fac, e.mfit, e.n_curves, e.row_stride);
+    int chosen = fits[0];
+    const char *source = "only layout that fits";
+    std::vector<float> ms(fits.size(), -1.0f);
+    if (fits.size() > 1 && mode == 0) {
+        source = "first that fits";
+    } else if (fits.size() > 1) {
+        bool cached = false;
+        {
+            std::lock_guard<std::mutex> lk(t.mu);
+            auto it = t.cache.find(key);
+            if (it != t.cache.end()) {
+                chosen = it->second;
+                cached = true;
+            }
+        }
+        source = "cache";
+        if (!cached) {
+            source = "timed";
+            float best = 0;
+            for (size_t c = 0; c < fits.size(); ++c) {
+                ps_status st = set_layout(fits[c]);
+                if (st == PS_OK) st = time_layout(b, g, &ms[c]);
+                if (st != PS_OK) return st;
+                if (c == 0 || ms[c] < best) {
+                    best = ms[c];
+                    chosen = fits[c];
+                }
+            }
+            std::lock_guard<std::mutex> lk(t.mu);
+            t.cache[key] = chosen;
         }
     }
-    if (!ok) return psb_fail(PS_ERR_ARG, "ps_gpu_scan_batch: objects too large for shared memory");
-    g.per_cta = 0;
-    for (int i : g.members) {
-        psb::DevObject o = b.h[i]->obj;
-        o.tile_rows = e.tile_rows;
-        o.cstat_smem = e.cstat_smem;
-        g.per_cta = std::max(g.per_cta, psb::fit_scratch_doubles(o));
+    ps_status st = set_layout(chosen);
+    if (st != PS_OK) return st;
+    char buf[256];
+    std::snprintf(buf, sizeof buf,
+                  "%s{\"ncp\": %d, \"objects\": %zu, \"n_fac\": %d, \"mfit\": %d, \"ctas\": %d, \"source\": \"%s\", "
+                  "\"chosen\": {\"tile_rows\": %d, \"cstat_smem\": %d}, \"candidates\": [",
+                  report.size() > 1 ? ", " : "", e.ncp, g.members.size(), e.n_fac, e.mfit, g.ctas, source,
+                  kLayouts[chosen][0], kLayouts[chosen][1]);
+    report += buf;
+    for (size_t c = 0; c < fits.size(); ++c) {
+        std::snprintf(buf, sizeof buf, "%s{\"tile_rows\": %d, \"cstat_smem\": %d, \"sample_ms\": %.4f}",
+                      c ? ", " : "", kLayouts[fits[c]][0], kLayouts[fits[c]][1], (double)ms[c]);
+        report += buf;
     }
-    const int per_sm = psb::fit_batch_ctas_per_sm(e);
-    if (per_sm < 1) return psb_fail(PS_ERR_CUDA, "ps_gpu_scan_batch: batch kernel cannot be resident");
-    g.ctas = per_sm * b.h[g.members[0]]->n_sm;
-    return PS_OK;
-}
-
-// The group's objects (their current constants) to the device.
-ps_status upload_objects(Batch &b, Group &g)
-{
-    std::vector<psb::DevObject> objs;
-    std::vector<psb::DevParams> prms;
-    for (int i : g.members) {
-        psb::DevObject o = b.h[i]->obj;
-        o.tile_rows = g.env.tile_rows;
-        o.cstat_smem = g.env.cstat_smem;
-        objs.push_back(o);
-        psb::DevParams p = b.h[i]->prm;
-        p.phase_cycles = nullptr;
-        prms.push_back(p);
-    }
-    PSB_CUDA(psb::upload(g.objs, objs, g.stream));
-    PSB_CUDA(psb::upload(g.prms, prms, g.stream));
+    report += "]}";
     return PS_OK;
 }
 
@@ -154,10 +301,11 @@ ps_status run_groups(Batch &b, const std::vector<std::vector<std::vector<psb::Fi
     for (size_t gi = 0; gi < b.groups.size(); ++gi) {
         Group &g = b.groups[gi];
         std::vector<psb::FitItem> flat;
-        for (size_t k = 0; k < g.members.size(); ++k) {
-            offset[gi].push_back((int)flat.size());
+        offset[gi].assign(g.members.size(), 0);
+        for (int k : g.order) {
+            offset[gi][k] = (int)flat.size();
             for (psb::FitItem it : items[gi][k]) {
-                it.pole |= (int)k << 8;
+                it.pole |= k << 8;
                 flat.push_back(it);
             }
         }
@@ -278,11 +426,17 @@ extern "C" ps_status ps_gpu_scan_batch(int32_t device, int32_t n_obj, const ps_o
         }
         b.groups[by_ncp[ncp]].members.push_back(i);
     }
+    std::string report = "[";
     for (Group &g : b.groups) {
         PSB_CUDA(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
         PSB_CUDA(cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming));
-        ps_status st = plan_group(b, g, prop.sharedMemPerBlockOptin);
+        ps_status st = plan_group(b, g, prop.sharedMemPerBlockOptin, report);
         if (st != PS_OK) return st;
+    }
+    report += "]";
+    {
+        std::lock_guard<std::mutex> lk(tuning().mu);
+        tuning().report = report;
     }
 
     // convexity-weight search, all objects' rounds together
@@ -371,4 +525,25 @@ extern "C" ps_status ps_gpu_scan_batch(int32_t device, int32_t n_obj, const ps_o
             n_lines[i] = nl;
         }
     return PS_OK;
+}
+
+extern "C" ps_status ps_batch_set_tuning(int32_t mode)
+{
+    if (mode != 0 && mode != 1) return psb_fail(PS_ERR_ARG, "ps_batch_set_tuning: mode must be 0 or 1");
+    std::lock_guard<std::mutex> lk(tuning().mu);
+    tuning().mode = mode;
+    if (mode == 1) tuning().cache.clear();
+    return PS_OK;
+}
+
+extern "C" int32_t ps_batch_tuning_report(char *buf, int32_t len)
+{
+    std::lock_guard<std::mutex> lk(tuning().mu);
+    const std::string &r = tuning().report;
+    if (buf && len > 0) {
+        const size_t n = std::min(r.size(), (size_t)len - 1);
+        std::memcpy(buf, r.data(), n);
+        buf[n] = 0;
+    }
+    return (int32_t)r.size();
 }

@@ -691,12 +691,15 @@ __device__ __forceinline__ uint32_t tf32_rna(float x)
     return r;
 }
 
-// Approximate FP32 reciprocal (the special-function unit's, no refinement).
-__device__ __forceinline__ float rcp_approx_f32(float x)
+// FP32 reciprocal: the special-function unit's approximation refined by one
+// Newton-Raphson step, r1 = r0 + r0 (1 - x r0), which brings its relative
+// error from about 2^-23 to the last bit or two of FP32.
+__device__ __forceinline__ float rcp_f32(float x)
 {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
+    const float e = fmaf(-x, r, 1.0f);
+    return fmaf(r, e, r);
 }
 
 // D += A B on the tensor cores, m16n8k8, TF32 operands, FP32 accumulation.
@@ -709,8 +712,10 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
 }
 
 // The facet sweep in mixed precision: the point geometry and the output rows
-// stay FP64; the per-facet Lambert + Lommel-Seeliger terms run in FP32 with
-// the per-point sums flushed into FP64 after every chunk of facets; the shape
+// stay FP64; the per-facet Lambert + Lommel-Seeliger terms run in FP32 (with
+// a Newton-refined reciprocal) and the per-point sums of each 8-facet step
+// are flushed into FP64 accumulators, so no FP32 sum runs over more than 8
+// terms; the shape
 // derivatives J = W Y run on the tensor cores as 3xTF32 products
 // (W_lo Y_hi + W_hi Y_lo + W_hi Y_hi, each operand split into a TF32 high
 // part and a TF32 remainder) with FP32 accumulation.  The chunk pipeline is
@@ -779,7 +784,6 @@ __device__ void brightness_rows_mixed(const DevObject &o, const Sh &s, double *r
                 const int f0 = c * fc, nfc = min(fc, nf - f0);
                 const float *yh = ybuf + (size_t)b * 2 * fc * NCP;
                 const float *yl = yh + fc * NCP;
-                float S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 1
                 for (int k0 = 0; k0 < nfc; k0 += 8) {
                     // visibility of the step's 8 facets, one vote
@@ -797,6 +801,7 @@ __device__ void brightness_rows_mixed(const DevObject &o, const Sh &s, double *r
                     }
                     const unsigned vm = __ballot_sync(0xffffffffu, v8);
                     if (!vm) continue;  // warp-uniform
+                    float S[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
                     uint32_t hi[8], lo[8];
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
@@ -809,7 +814,7 @@ __device__ void brightness_rows_mixed(const DevObject &o, const Sh &s, double *r
                         const float4 fr = s.F32[fq];
                         const float2 ls = s.G32[fq];
                         const float mv = vis[q] ? mu[q] : 0.0f, m0v = vis[q] ? mu0[q] : 0.0f;
-                        const float r = rcp_approx_f32(vis[q] ? mu[q] + mu0[q] : 1.0f);
+                        const float r = rcp_f32(vis[q] ? mu[q] + mu0[q] : 1.0f);
                         const float z = fr.w * (mv * m0v);
                         const float zr = z * r;
                         const float w = fmaf(cls, zr, cl * z);
@@ -828,6 +833,8 @@ __device__ void brightness_rows_mixed(const DevObject &o, const Sh &s, double *r
                         hi[q] = tf32_rna(w);
                         lo[q] = tf32_rna(w - __uint_as_float(hi[q]));
                     }
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) S64[i] += (double)S[i];
                     // this lane's row of the step's weight tile, high and low parts
                     uint4 *ph = reinterpret_cast<uint4 *>(whi + lane * kWS);
                     uint4 *pl = reinterpret_cast<uint4 *>(wlo + lane * kWS);
@@ -871,8 +878,6 @@ __device__ void brightness_rows_mixed(const DevObject &o, const Sh &s, double *r
                     }
                     __syncwarp();
                 }
-#pragma unroll
-                for (int i = 0; i < 9; ++i) S64[i] += (double)S[i];
             }
             // release the buffer; the last of the kWarps warps refills it
             __syncwarp();

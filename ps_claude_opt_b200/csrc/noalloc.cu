@@ -14,11 +14,18 @@
 // the call allocates nothing, on the device or on the host heap.
 //
 // Contract (also in include/ps_b200.h):
-//   * the arena is kNoAllocArenaBytes on every device that loads the library,
-//     held until the process exits;
-//   * the first call on a device looks up the arena's device address with
-//     that device current (cudaGetSymbolAddress) and sets the kernel's
-//     shared-memory limit; make that first call before any stream capture;
+//   * the arena is kNoAllocArenaBytes per device, reserved when this file's
+//     module first loads on that device and held until the process exits.
+//     CUDA loads modules lazily, so the reservation happens inside the first
+//     call on the device, which may fail if the device is already full by
+//     then; a call with n = 0 does only that (select the device, load the
+//     module, look up the arena) and lets a caller reserve the arena at start
+//     time, before its own allocator grows;
+//   * every call looks up the arena's device address with the device current
+//     (cudaGetSymbolAddress: cheap once the module is loaded, and never stale
+//     after a cudaDeviceReset); the first call with work also sets the fit
+//     kernel's shared-memory limit; make the first call before any stream
+//     capture;
 //   * every call reuses the arena and leaves the last call's contents there;
 //     calls that overlap on the GPU (two host threads, or two streams) race
 //     on it -- serialise them;
@@ -44,19 +51,16 @@ constexpr int kMaxIterCap = 60;   // constants.h:12
 
 static __device__ __align__(256) unsigned char g_arena[kNoAllocArenaBytes];
 
-// Device address of g_arena per device, looked up once with that device current.
-unsigned char *g_arena_addr[kMaxDevices];
-
-ps_status arena_for(int device, unsigned char **out)
+// Device address of g_arena on the current device.  In host code g_arena
+// names a host-side shadow, not device memory, so the kernels get this
+// address.  Looked up on every call: cheap once the module is loaded, and a
+// cached address would go stale if the host reset the device.
+ps_status arena_address(unsigned char **out)
 {
-    if (device < 0 || device >= kMaxDevices) return psb_fail(PS_ERR_ARG, "ps_fit_items_noalloc: device index");
-    if (!g_arena_addr[device]) {
-        void *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_arena);
-        if (e != cudaSuccess) return psb_fail_cuda(e, "cudaGetSymbolAddress(arena)");
-        g_arena_addr[device] = static_cast<unsigned char *>(ptr);
-    }
-    *out = g_arena_addr[device];
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_arena);
+    if (e != cudaSuccess) return psb_fail_cuda(e, "cudaGetSymbolAddress(arena)");
+    *out = static_cast<unsigned char *>(ptr);
     return PS_OK;
 }
 
@@ -104,11 +108,19 @@ extern "C" ps_status ps_fit_items_noalloc(
     int32_t numfac, const double *brightness, const ps_curves *curves, const ps_shape *shape, int32_t n,
     const int32_t *n_freq, const int32_t *pole, ps_fit_result *out)
 {
+    if (device < 0 || device >= kMaxDevices || n < 0)
+        return psb_fail(PS_ERR_ARG, "ps_fit_items_noalloc: device index or n < 0");
+    if (n == 0) {
+        // warm-up: select the device and load this module there, which
+        // reserves the arena; nothing else is read or launched
+        NA_CUDA(cudaSetDevice(device));
+        unsigned char *arena = nullptr;
+        return arena_address(&arena);
+    }
     if (!beta_pole || !lambda_pole || !par || !ee || !ee0 || !tim || !weight || !ia || !ia_par || !cg_first ||
         !sig || !sigr2 || !brightness || !curves || !shape || !curves->curve_len || !curves->curve_rel ||
-        !shape->normal || !shape->d_area || !shape->d_sphere || n < 0 || (n > 0 && (!n_freq || !pole || !out)))
+        !shape->normal || !shape->d_area || !shape->d_sphere || !n_freq || !pole || !out)
         return psb_fail(PS_ERR_ARG, "ps_fit_items_noalloc: null argument");
-    if (n == 0) return PS_OK;
     if (!(cl > 0) || ndata <= 0 || !(freq_step > 0))
         return psb_fail(PS_ERR_ARG, "ps_fit_items_noalloc: cl, ndata and freq_step must be > 0");
     const int nc = shape->n_coef, ma = nc + 8, nfac = numfac, ncur = curves->n_curves;
@@ -143,22 +155,24 @@ extern "C" ps_status ps_fit_items_noalloc(
 
     NA_CUDA(cudaSetDevice(device));
     unsigned char *arena = nullptr;
-    ps_status st = arena_for(device, &arena);
+    ps_status st = arena_address(&arena);
     if (st != PS_OK) return st;
-    cudaDeviceProp prop;
-    NA_CUDA(cudaGetDeviceProperties(&prop, device));
+    int smem_optin = 0, n_sm = 0;
+    NA_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    NA_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, device));
+    const size_t smem_limit = (size_t)smem_optin;
     int tile_rows = 32, cstat_smem = 1;
     const int rs = (ma + 2) & ~1;
     size_t smem = psb::fit_smem_bytes(nfac, mfit, ncp, ncur, rs, tile_rows, cstat_smem, 0);
-    if (smem > prop.sharedMemPerBlockOptin) {
+    if (smem > smem_limit) {
         cstat_smem = 0;
         smem = psb::fit_smem_bytes(nfac, mfit, ncp, ncur, rs, tile_rows, cstat_smem, 0);
     }
-    if (smem > prop.sharedMemPerBlockOptin) {
+    if (smem > smem_limit) {
         tile_rows = 16;
         smem = psb::fit_smem_bytes(nfac, mfit, ncp, ncur, rs, tile_rows, cstat_smem, 0);
     }
-    if (smem > prop.sharedMemPerBlockOptin)
+    if (smem > smem_limit)
         return psb_fail(PS_ERR_ARG, "ps_fit_items_noalloc: object too large for shared memory");
 
     // arena layout
@@ -272,7 +286,7 @@ extern "C" ps_status ps_fit_items_noalloc(
     const int per_sm = psb::fit_ctas_per_sm(o);
     if (per_sm < 1) return psb_fail(PS_ERR_CUDA, "ps_fit_items_noalloc: fit kernel cannot be resident");
     const size_t fit_scratch = (kNoAllocArenaBytes - o_scratch) / per_cta;
-    int n_ctas = per_sm * prop.multiProcessorCount;
+    int n_ctas = per_sm * n_sm;
     if ((size_t)n_ctas > fit_scratch) n_ctas = (int)fit_scratch;
     if (n_ctas > n) n_ctas = n;
     int *ctl = reinterpret_cast<int *>(arena + o_ctl);

@@ -94,6 +94,8 @@ _SIGS = {
     "ps_gpu_scan_batch": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(Object), C.c_int32, C.POINTER(Line),
                                     C.POINTER(C.c_int64), _ip, _dp]),
     "ps_gpu_set_precision": (C.c_int, [C.c_void_p, C.c_int32]),
+    "ps_batch_set_tuning": (C.c_int, [C.c_int32]),
+    "ps_batch_tuning_report": (C.c_int32, [C.c_char_p, C.c_int32]),
     "ps_screen_features": (C.c_int, [C.c_int32, C.c_int32, _dp, _dp, C.POINTER(Curves), C.c_int32, _dp,
                                      C.POINTER(C.c_float)]),
     "ps_screen_rank": (C.c_int, [C.c_int32, C.c_int32, _dp, _dp, C.POINTER(Curves), C.c_int32, _dp, C.c_int32,
@@ -369,6 +371,16 @@ def fit_items_noalloc(obj, n_freq, pole, device=0, conw_r=None):
     return out.reshape(n, 6), niter, status
 
 
+def reserve_noalloc(device=0):
+    """ps_fit_items_noalloc with no work (n = 0, every array NULL): selects
+    the device and loads the library's module there, which reserves the
+    entry point's static device arena.  Call it at start-up, before another
+    allocator fills the device."""
+    _check(lib().ps_fit_items_noalloc(device, None, None, None, None, 0.0, 0.0, 0.0, 0.0, None, None, None, 0.0,
+                                      None, 0.0, 0.0, 0.0, 0, 0.0, 0.0, 0, None, None, None, None, None, 0, None,
+                                      None, None, 0, None, None, None))
+
+
 def scan_batch(objs, device=0, quirks=0, max_freq=None):
     """ps_gpu_scan_batch over prepared objects: each object's convexity-weight
     search and scan, all on one GPU at once.  Returns [(lines, conw_r)] in the
@@ -415,6 +427,22 @@ def scan_batch(objs, device=0, quirks=0, max_freq=None):
         out.append((np.array([(l.period_h, l.rms, l.chisq, l.dark, l.lambda_deg, l.beta_deg) for l in ls]),
                     float(cw[i])))
     return out
+
+
+def batch_set_tuning(mode):
+    """ps_batch_set_tuning: 1 = autotuned tile layouts (default), 0 = the
+    first layout that fits."""
+    _check(lib().ps_batch_set_tuning(int(mode)))
+
+
+def batch_tuning_report():
+    """The last scan_batch's per-group layout choices (parsed JSON)."""
+    import json
+
+    n = lib().ps_batch_tuning_report(None, 0)
+    buf = C.create_string_buffer(n + 1)
+    lib().ps_batch_tuning_report(buf, n + 1)
+    return json.loads(buf.value.decode())
 
 
 def run_object(obj, device=0, quirks=0, max_freq=None, progress=None, precision=PRECISION_FP64):

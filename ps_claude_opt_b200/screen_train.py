@@ -173,6 +173,49 @@ def judge(net, fulls, top=0.034, halo=1, audit=0.02, log=print, precision=native
     return hits, rows
 
 
+def judge_stream(net, start, count, out_path, precision=native.PRECISION_MIXED, fp64_every=10, log=print):
+    """The held-out judgement at scale, one JSON line per object appended to
+    out_path as soon as it is done (a partial run keeps its rows): the full
+    scan of object EVAL_SEED + start + i in `precision` (the judge), the
+    screened scan in the same precision with its plan (edge expansions,
+    fallback), and for every `fp64_every`-th object also the plain FP64
+    full scan, to check that the cheaper judge names the same best line."""
+    done = set()
+    try:
+        with open(out_path) as f:
+            done = {json.loads(l)["seed"] for l in f if l.strip()}
+    except FileNotFoundError:
+        pass
+    for i in range(start, start + count):
+        seed = EVAL_SEED + i
+        if seed in done:
+            continue
+        obj, truth = make_object(seed)
+        t0 = time.time()
+        full, conw_r = native.run_object(obj, precision=precision)
+        t_full = time.time() - t0
+        t0 = time.time()
+        idx, lines, _, plan = screen.screened_scan(obj, net, conw_r, seed=i, precision=precision)
+        t_scr = time.time() - t0
+        bf, bs = screen.best_line(full), screen.best_line(lines)
+        row = dict(seed=seed, n_freq=len(full), conw_r=conw_r, full_best=bf + 1, full_line=[float(v) for v in full[bf]],
+                   screened_best=int(idx[bs]), screened_line=[float(v) for v in lines[bs]],
+                   same_line=bool(idx[bs] == bf + 1 and np.array_equal(lines[bs], full[bf])),
+                   fitted=int(len(idx)), initial=plan.initial, expansions=plan.expansions,
+                   fallback=plan.fallback, reason=plan.reason, full_s=t_full, screened_s=t_scr,
+                   true_period_h=float(truth["period_h"]), precision=int(precision))
+        if fp64_every and (i - start) % fp64_every == 0 and precision != native.PRECISION_FP64:
+            t0 = time.time()
+            f64, cw64 = native.run_object(obj)
+            b64 = screen.best_line(f64)
+            row.update(fp64_best=b64 + 1, fp64_line=[float(v) for v in f64[b64]], fp64_s=time.time() - t0,
+                       judge_agrees_with_fp64=bool(b64 == bf and native.format_lines(f64[b64:b64 + 1]) ==
+                                                   native.format_lines(full[bf:bf + 1])))
+        with open(out_path, "a") as f:
+            f.write(json.dumps(row) + "\n")
+        log(json.dumps(row))
+
+
 def main():
     import os
 
@@ -185,7 +228,13 @@ def main():
     ap.add_argument("--eval-start", type=int, default=0, help="first held-out object (seed offset)")
     ap.add_argument("--model", default=None, help="judge this trained network instead of training one")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--judge-out", default=None,
+                    help="stream the held-out judgement (mixed-precision judge) to this JSON-lines file")
     args = ap.parse_args()
+    if args.judge_out:
+        net = screen.load_model(args.model or screen.MODEL_PATH)
+        judge_stream(net, args.eval_start, args.eval_objects, args.judge_out)
+        return
     t0 = time.time()
     if args.model:
         net = screen.load_model(args.model)

@@ -278,3 +278,46 @@ def config3_object(i: int, seed0: int = 1000003 * 3):
 
 
 C3_OBJECTS = 64
+
+
+def config3_object(i: int, seed0: int = 1000003 * 3):
+    """Object i of the batched workload: points log-uniform in 300..19 900
+    (relative curves of equal length, at most 199 of them -- with the
+    pseudo-curve the reference's MAX_LC of 200), lmax = mmax in {4, 6, 8},
+    nrows in {6, 8, 10}, trial-frequency count log-uniform in 500..20 000
+    around the true period, stop condition 0.005 (fits run until the rms
+    improves by less than that: ragged iteration counts).  Returns
+    (SynthConfig, seed)."""
+    rng = np.random.default_rng(seed0 + i)
+    n_pts = int(round(math.exp(rng.uniform(math.log(300), math.log(19900)))))
+    lmax = int(rng.choice([4, 6, 8]))
+    nrows = int(rng.choice([6, 8, 10]))
+    n_freq = int(round(math.exp(rng.uniform(math.log(500), math.log(20000)))))
+    n_curves = min(199, max(5, n_pts // 80))
+    per = max(1, n_pts // n_curves)
+    cfg = SynthConfig(l_max=lmax, m_max=lmax, nrows=nrows, n_dense=n_curves, dense_pts=(per, per),
+                      n_freq=n_freq, stop_condition=0.005, n_iter_min=10)
+    return cfg, seed0 + i
+
+
+C3_OBJECTS = 64
+
+# The two inputs both the reference's own GPU application and this project's
+# host program are run on (golden files, parity tests, the bench's
+# reference_gpu leg): BASELINE config 1 object 0 and the relative-only
+# production object, each with the neutral trailing weight line.
+REFERENCE_INPUTS = {"c1": (C1, 1000003 * 1), "c2rel": (C2_REL, 1000003 * 2)}
+
+
+def reference_input_text(name: str, one_freq: bool = False) -> str:
+    """period_search_in text of REFERENCE_INPUTS[name]; one_freq=True gives
+    the same input with period end = period start, a grid of one frequency
+    (its wall time is the program's fixed cost: start-up, tables and the
+    convexity-weight search)."""
+    cfg, seed = REFERENCE_INPUTS[name]
+    text, _ = generate(cfg, seed)
+    if one_freq:
+        first, rest = text.split("\n", 1)
+        p = first.split()
+        text = "%s %s %s %s  period start/step/stop (free)\n%s" % (p[0], p[1], p[0], p[3], rest)
+    return text + NEUTRAL_WEIGHT_LINE

@@ -42,18 +42,7 @@ sys.path.insert(0, ROOT)
 
 from ps_claude_opt_b200 import compare, synth  # noqa: E402
 
-SEEDS = {"c1": 1000003 * 1, "c2rel": 1000003 * 2}
-CONFIGS = {"c1": synth.C1, "c2rel": synth.C2_REL}
-
-
-def input_text(name: str, one_freq: bool = False) -> str:
-    text, _ = synth.generate(CONFIGS[name], SEEDS[name])
-    if one_freq:
-        first, rest = text.split("\n", 1)
-        p = first.split()
-        # period end = period start: the grid holds exactly one frequency
-        text = "%s %s %s %s  period start/step/stop (free)\n%s" % (p[0], p[1], p[0], p[3], rest)
-    return text + synth.NEUTRAL_WEIGHT_LINE
+input_text = synth.reference_input_text
 
 
 def run(cmd, text, timeout):
