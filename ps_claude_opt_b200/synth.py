@@ -40,6 +40,7 @@ class SynthConfig:
     n_iter_min: int = 10
     conw: float = 0.1
     r_ast: float = 2.0
+    truth_grid: tuple = (60, 120)   # (theta, phi) cells of the direction grid the truth brightness sums over
 
 
 C1 = SynthConfig()
@@ -104,7 +105,7 @@ def generate(cfg: SynthConfig, seed: int):
     phi0 = rng.uniform(0, 2 * math.pi)
     cl_true, pA, pD, pK = 0.1, 0.5, 0.1, -0.5
 
-    T, P, dom, nrm = _truth_grid()
+    T, P, dom, nrm = _truth_grid(*cfg.truth_grid)
     area = dom * np.exp(_basis(cfg.l_max, cfg.m_max, T, P) @ coef)
 
     # orbit geometry (ecliptic frame): asteroid circular orbit, inclined
@@ -272,8 +273,10 @@ def config3_object(i: int, seed0: int = 1000003 * 3):
     n_freq = int(round(math.exp(rng.uniform(math.log(500), math.log(20000)))))
     n_curves = min(199, max(5, n_pts // 80))
     per = max(1, n_pts // n_curves)
+    # the truth sums over 30 x 60 directions (1800, still finer than the
+    # fits' 288-800 facets) to keep generating 64 objects short
     cfg = SynthConfig(l_max=lmax, m_max=lmax, nrows=nrows, n_dense=n_curves, dense_pts=(per, per),
-                      n_freq=n_freq, stop_condition=0.005, n_iter_min=10)
+                      n_freq=n_freq, stop_condition=0.005, n_iter_min=10, truth_grid=(30, 60))
     return cfg, seed0 + i
 
 
@@ -295,8 +298,10 @@ def config3_object(i: int, seed0: int = 1000003 * 3):
     n_freq = int(round(math.exp(rng.uniform(math.log(500), math.log(20000)))))
     n_curves = min(199, max(5, n_pts // 80))
     per = max(1, n_pts // n_curves)
+    # the truth sums over 30 x 60 directions (1800, still finer than the
+    # fits' 288-800 facets) to keep generating 64 objects short
     cfg = SynthConfig(l_max=lmax, m_max=lmax, nrows=nrows, n_dense=n_curves, dense_pts=(per, per),
-                      n_freq=n_freq, stop_condition=0.005, n_iter_min=10)
+                      n_freq=n_freq, stop_condition=0.005, n_iter_min=10, truth_grid=(30, 60))
     return cfg, seed0 + i
 
 
