@@ -39,11 +39,11 @@ ROOT = os.path.dirname(HERE)
 sys.path.insert(0, GOLDEN)
 
 
-def _run_host(name, tmp_path, precision="fp64", program=None):
+def _run_host(name, tmp_path, precision="fp64", program=None, tag=None):
     from make_refapp_golden import input_text
     from ps_claude_opt_b200 import native
 
-    d = tmp_path / ("%s_%s" % (name, precision))
+    d = tmp_path / ("%s_%s" % (name, tag or precision))
     d.mkdir()
     (d / "period_search_in").write_text(input_text(name))
     cmd = program or [native.HOST_PROGRAM, "--fresh", "--precision", precision]
@@ -94,7 +94,7 @@ def test_reference_main_on_the_b200_engine(tmp_path):
     shim = os.path.join(ROOT, "oracle", "_ref", "refapp_b200shim")
     if not os.path.exists(shim):
         pytest.skip("refapp_b200shim not built (oracle/refapp/build.sh needs the reference source tree)")
-    a = _run_host("c1", tmp_path, program=[shim, "--device", "0"])
+    a = _run_host("c1", tmp_path, program=[shim, "--device", "0"], tag="refmain")
     b = _run_host("c1", tmp_path, precision="fp64")
     assert open(a).read() == open(b).read()
 
