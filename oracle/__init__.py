@@ -65,8 +65,11 @@ def build(quiet: bool = True) -> None:
 _LIBS: dict = {}
 
 
-def lib(fast: bool = False) -> C.CDLL:
-    name = "libps_oracle_fast.so" if fast else "libps_oracle.so"
+def lib(fast: bool = False, fma: bool = False) -> C.CDLL:
+    """The strict oracle; fast=True the -O3 -march=native build (timed CPU
+    baseline); fma=True the build with FMA contraction (the same algorithm
+    under a different rounding)."""
+    name = "libps_oracle_fma.so" if fma else ("libps_oracle_fast.so" if fast else "libps_oracle.so")
     if name not in _LIBS:
         path = os.path.join(BUILD, name)
         if not os.path.exists(path):
@@ -229,8 +232,8 @@ def gauss_solve(a, b):
     return rc, b
 
 
-def run_file(in_path, out_path, quirks=0, threads=0, max_freq=0):
-    rc = lib().pso_run_file(in_path.encode(), out_path.encode(), quirks, threads or os.cpu_count() or 1,
+def run_file(in_path, out_path, quirks=0, threads=0, max_freq=0, fma=False):
+    rc = lib(fma=fma).pso_run_file(in_path.encode(), out_path.encode(), quirks, threads or os.cpu_count() or 1,
                             max_freq)
     if rc != 0:
         raise RuntimeError(f"oracle run failed ({rc})")

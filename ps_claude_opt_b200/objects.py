@@ -93,6 +93,24 @@ def _tokens(line: str):
     return line.split()
 
 
+def scan_grid(text: str) -> ScanGrid:
+    """The trial-frequency grid of a period_search_in text without preparing
+    the object: 1/P_start, 1/P_end and 0.5 coef / (24 (JD_max - JD_min))
+    (period_search_BOINC.cpp:839-841)."""
+    lines = text.splitlines()
+    p_start, p_coef, p_end = (float(v) for v in _tokens(lines[0])[:3])
+    rest = " ".join(lines[14:]).split()
+    pos, jd_min, jd_max = 1, math.inf, -math.inf
+    for _ in range(int(rest[0])):
+        lp = int(rest[pos])
+        pos += 2
+        for j in range(lp):
+            t = float(rest[pos + 8 * j])
+            jd_min, jd_max = min(jd_min, t), max(jd_max, t)
+        pos += 8 * lp
+    return ScanGrid(1 / p_start, 1 / p_end, 0.5 / (jd_max - jd_min) / 24 * p_coef)
+
+
 def parse_input(text: str, setup_fn=None) -> PreparedObject:
     """Parses a period_search_in text and prepares the object."""
     lines = text.splitlines()

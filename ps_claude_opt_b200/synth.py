@@ -314,15 +314,29 @@ C3_OBJECTS = 64
 REFERENCE_INPUTS = {"c1": (C1, 1000003 * 1), "c2rel": (C2_REL, 1000003 * 2)}
 
 
-def reference_input_text(name: str, one_freq: bool = False) -> str:
-    """period_search_in text of REFERENCE_INPUTS[name]; one_freq=True gives
-    the same input with period end = period start, a grid of one frequency
-    (its wall time is the program's fixed cost: start-up, tables and the
-    convexity-weight search)."""
+def reference_input_text(name: str, one_freq: bool = False, stop: float | None = None,
+                         n_freq: int | None = None) -> str:
+    """period_search_in text of REFERENCE_INPUTS[name].  one_freq=True sets
+    period end = period start, a grid of one frequency (its wall time is the
+    program's fixed cost: start-up, tables and the convexity-weight search);
+    n_freq moves the period end so the same grid (same start and step) holds
+    n_freq frequencies; stop replaces the stop condition (e.g. 5: exactly 5
+    LM iterations per fit)."""
     cfg, seed = REFERENCE_INPUTS[name]
     text, _ = generate(cfg, seed)
+    first, rest = text.split("\n", 1)
+    p = first.split()
     if one_freq:
-        first, rest = text.split("\n", 1)
-        p = first.split()
-        text = "%s %s %s %s  period start/step/stop (free)\n%s" % (p[0], p[1], p[0], p[3], rest)
+        p[2] = p[0]
+    elif n_freq is not None:
+        from .objects import scan_grid
+
+        g = scan_grid(text)
+        p[2] = "%.17g" % (1.0 / (g.freq_start - (n_freq - 0.5) * g.freq_step))
+    text = "%s %s %s %s  period start/step/stop (free)\n%s" % (p[0], p[1], p[2], p[3], rest)
+    if stop is not None:
+        lines = text.splitlines(True)
+        k = [i for i, l in enumerate(lines) if "stop condition" in l][0]
+        lines[k] = "%g  stop condition\n" % stop
+        text = "".join(lines)
     return text + NEUTRAL_WEIGHT_LINE

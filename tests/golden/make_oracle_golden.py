@@ -7,13 +7,15 @@ only; the oracle is the strict FP64 build, identical on every x86-64 host).
                   gives the reference's GPU app
   c2rel_scan.out  the same for the production object without calibrated
                   points, 200 frequencies around the true period
+  c1_stop5_scan.out, c2rel_stop{3,10,20}_scan.out
+                  the same inputs cut to 5, 3, 10 and 20 LM iterations
   c2_fits.npz     50-iteration fits of the production object (with its 400
                   calibrated points) at 20 frequencies x 10 poles: the 10
                   grid frequencies nearest the true period and 10 spread
                   over the 2-100 h grid; per fit (rms, dark, period,
                   lambda, beta, chi^2), iteration count and status
 
-    python tests/golden/make_oracle_golden.py [c1] [c2rel] [c2fits]
+    python tests/golden/make_oracle_golden.py [c1] [c2rel] [c2fits] [stops]
 
 A few minutes on 8 cores (c1 ~80 s, c2rel ~5 min, c2fits ~1 min).
 """
@@ -50,12 +52,12 @@ def c2_fit_items(obj, truth):
     return nf, pl
 
 
-def scan(name):
+def scan(name, stop=None):
     with tempfile.TemporaryDirectory() as d:
         inp = os.path.join(d, "period_search_in")
         with open(inp, "w") as f:
-            f.write(input_text(name))
-        out = os.path.join(OUT, "%s_scan.out" % name)
+            f.write(input_text(name, stop=stop))
+        out = os.path.join(OUT, "%s%s_scan.out" % (name, "" if stop is None else "_stop%d" % stop))
         oracle.run_file(inp, out)
     print("wrote", out)
 
@@ -72,10 +74,14 @@ def c2fits():
 
 def main(argv):
     os.makedirs(OUT, exist_ok=True)
-    todo = argv or ["c1", "c2rel", "c2fits"]
+    todo = argv or ["c1", "c2rel", "c2fits", "stops"]
     for t in todo:
         if t == "c2fits":
             c2fits()
+        elif t == "stops":
+            scan("c1", 5)
+            for k in (3, 10, 20):
+                scan("c2rel", k)
         else:
             scan(t)
 

@@ -1,12 +1,12 @@
 """Runs the reference's own GPU application and this project's host program
 on the same inputs, and keeps the reference's output files as golden
-fixtures.
+fixtures (tests/golden/refapp/).
 
 The reference app is built (unchanged, against the project's BOINC stub) by
 ``oracle/refapp/build.sh`` into ``oracle/_ref/refapp_sm100a`` (native sm_100a)
 and ``oracle/_ref/refapp_lto100`` (the reference Makefile's own sm_100 entry,
 compute_100 LTO-IR + sm_100).  Needs a B200.  Inputs are regenerated from
-their seeds:
+their seeds (ps_claude_opt_b200.synth.reference_input_text):
 
   c1     BASELINE config 1 object 0: lmax 3, 288 facets, 20 x 60 relative
          points, 200 trial frequencies around the true period (2000 fits)
@@ -15,15 +15,14 @@ their seeds:
          code skips the brightness of calibrated curves, so it is an oracle
          only for relative data -- on 200 frequencies around the true period
 
-Each program also runs on a one-frequency copy of each input, so the fixed
-cost (start-up, tables, convexity-weight search) can be subtracted from the
-scan's wall time.
+Files written to OUTDIR:
+  refapp_<build>_<input>.out         50 LM iterations (the inputs' stop condition)
+  refapp_sm100a_<input>_stop<k>.out  the same input cut to k LM iterations
+  refapp_sm100a_c2rel_run<r>.out     repeated runs of the same input and binary
+  ours_<precision>_<input>.out       this project's host program, for comparison
+  summary.json                       wall times, comparisons
 
-    python tests/golden/make_refapp_golden.py OUTDIR [--only c1,c2rel] [--variants sm100a,lto100]
-
-Writes OUTDIR/<variant>_<input>.out, OUTDIR/ours_<precision>_<input>.out,
-their stdout/stderr tails and OUTDIR/summary.json.  The committed fixtures in
-tests/golden/refapp/ are copies of OUTDIR/refapp_sm100a_<input>.out.
+    python tests/golden/make_refapp_golden.py OUTDIR
 """
 from __future__ import annotations
 
@@ -105,6 +104,19 @@ def main():
                 c = compare.compare_files(os.path.join(args.outdir, "%s_%s.out" % (prog, name)), ref_path)
                 summary["%s_%s" % (prog, name)]["vs_refapp_sm100a"] = c.as_dict()
                 print("  %s vs refapp_sm100a: %s" % (prog, c.summary()), flush=True)
+    app = progs.get("refapp_sm100a")
+    if app:
+        for name, stops in (("c1", (5,)), ("c2rel", (2, 3, 5, 10))):
+            for k in stops:
+                rc, w, out, _, _ = run(app, input_text(name, stop=k), args.timeout)
+                with open(os.path.join(args.outdir, "refapp_sm100a_%s_stop%d.out" % (name, k)), "w") as f:
+                    f.write(out)
+                summary["refapp_sm100a_%s_stop%d" % (name, k)] = {"rc": rc, "wall_s": w}
+        for r in range(2, 5):
+            rc, w, out, _, _ = run(app, input_text("c2rel"), args.timeout)
+            with open(os.path.join(args.outdir, "refapp_sm100a_c2rel_run%d.out" % r), "w") as f:
+                f.write(out)
+            summary["refapp_sm100a_c2rel_run%d" % r] = {"rc": rc, "wall_s": w}
     with open(os.path.join(args.outdir, "summary.json"), "w") as f:
         json.dump(summary, f, indent=1)
 
