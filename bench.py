@@ -82,19 +82,24 @@ def bench_batch(texts, max_freq, device=0):
     objs = [objects.parse_input(t) for t in texts]
     t_setup = time.perf_counter() - t0
     out = {}
-    native.batch_set_tuning(1)
+    native.batch_set_tuning(2)
     t0 = time.perf_counter()
     tuned_first = native.scan_batch(objs, device=device, max_freq=max_freq)
     out["tuned_first_call_s"] = time.perf_counter() - t0   # includes timing the candidate layouts
     report = native.batch_tuning_report()
-    t0 = time.perf_counter()
-    tuned = native.scan_batch(objs, device=device, max_freq=max_freq)
-    out["tuned_s"] = time.perf_counter() - t0               # layouts from the cache
-    native.batch_set_tuning(0)
-    t0 = time.perf_counter()
-    first_fit = native.scan_batch(objs, device=device, max_freq=max_freq)
-    out["first_fit_s"] = time.perf_counter() - t0
-    native.batch_set_tuning(1)
+    tuned_t, first_t = [], []
+    for _ in range(2):   # alternate the two forms; keep each one's fastest call
+        t0 = time.perf_counter()
+        tuned = native.scan_batch(objs, device=device, max_freq=max_freq)   # layouts from the cache
+        tuned_t.append(time.perf_counter() - t0)
+        native.batch_set_tuning(0)
+        t0 = time.perf_counter()
+        first_fit = native.scan_batch(objs, device=device, max_freq=max_freq)
+        first_t.append(time.perf_counter() - t0)
+        first_report = native.batch_tuning_report()
+        native.batch_set_tuning(1)
+    out["tuned_s"], out["first_fit_s"] = min(tuned_t), min(first_t)
+    out["first_fit_layouts"] = [g["chosen"] for g in first_report]
     t0 = time.perf_counter()
     one = [native.run_object(o, device=device, max_freq=max_freq) for o in objs]
     out["one_by_one_s"] = time.perf_counter() - t0
@@ -140,15 +145,15 @@ def run_program(cmd, text, timeout=1200):
         shutil.rmtree(d, ignore_errors=True)
 
 
-def program_scan_rate(cmd, name):
-    """Scan fits/s of a period_search-style program on REFERENCE_INPUTS[name]:
-    (lines - 1) x 10 fits / (wall time of the whole input - wall time of its
-    one-frequency copy), which takes start-up, tables and the
-    convexity-weight search out of both."""
+def program_scan_rate(cmd, name, n_freq=None):
+    """Scan fits/s of a period_search-style program on REFERENCE_INPUTS[name]
+    (its grid extended to n_freq frequencies): (lines - 1) x 10 fits / (wall
+    time of the whole input - wall time of its one-frequency copy), which
+    takes start-up, tables and the convexity-weight search out of both."""
     from ps_claude_opt_b200 import synth
 
     rc1, w1, _ = run_program(cmd, synth.reference_input_text(name, one_freq=True))
-    rc, w, lines = run_program(cmd, synth.reference_input_text(name))
+    rc, w, lines = run_program(cmd, synth.reference_input_text(name, n_freq=n_freq))
     ok = rc == 0 and rc1 == 0 and len(lines) > 1 and w > w1
     fits = 10 * (len(lines) - 1)
     return {"rc": rc, "wall_s": w, "wall_one_freq_s": w1, "lines": len(lines),
@@ -156,29 +161,33 @@ def program_scan_rate(cmd, name):
             "s_per_object_scan": (w - w1) if ok else None}, lines
 
 
-def reference_gpu_leg(names=("c1", "c2rel")):
+def reference_gpu_leg(grids=(("c1", 2000), ("c2rel", 1000))):
     """The reference's own GPU application (unchanged, sm_100a build) and
     this project's host program on the same inputs and the same B200, timed
-    the same way (program_scan_rate), with the comparator's verdict of our
-    lines against the reference's."""
+    the same way (program_scan_rate; config 1 on 2000 frequencies, the
+    relative-only production object on 1000, so the scan outweighs the
+    fixed cost), with the comparator's counts of our lines against the
+    reference's (whose 50-iteration lines are not repeatable run to run)."""
     from ps_claude_opt_b200 import compare, native
 
     app = os.path.join(ROOT, "oracle", "_ref", "refapp_sm100a")
     if not os.path.exists(app):
         return {"unavailable": "oracle/_ref/refapp_sm100a not built (oracle/refapp/build.sh)"}
     out = {}
-    for name in names:
-        ref, ref_lines = program_scan_rate([app, "--device", "0"], name)
-        ours, our_lines = program_scan_rate([native.HOST_PROGRAM, "--fresh"], name)
+    for name, n_freq in grids:
+        ref, ref_lines = program_scan_rate([app, "--device", "0"], name, n_freq)
+        ours, our_lines = program_scan_rate([native.HOST_PROGRAM, "--fresh"], name, n_freq)
         c = compare.compare_lines(our_lines, ref_lines)
-        out[name] = {"reference_app": ref, "ours_host_program": ours,
+        out[name] = {"frequencies": n_freq, "fits": 10 * n_freq, "reference_app": ref, "ours_host_program": ours,
                      "speedup_scan": (ours["scan_fits_per_s"] / ref["scan_fits_per_s"])
                      if ours["scan_fits_per_s"] and ref["scan_fits_per_s"] else None,
                      "speedup_whole_program": ref["wall_s"] / ours["wall_s"] if ours["wall_s"] else None,
                      "lines_vs_reference": {"pole_or_dark_mismatches": c.pole_mismatch, "worst": list(c.worst),
                                             "outside_envelope": c.envelope_violations,
                                             "best_line_same": c.best_line_same, "identical": c.identical,
-                                            "n_lines": c.n_lines}}
+                                            "n_lines": c.n_lines, "mean_rms_ours": c.mean_rms_test,
+                                            "mean_rms_reference": c.mean_rms_ref,
+                                            "reference_nan_lines": c.nan_ref}}
     return out
 
 

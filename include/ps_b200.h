@@ -164,9 +164,9 @@ ps_status ps_gpu_scan_batch(int32_t device, int32_t n_obj, const ps_object *objs
    mode 1 (default) times every layout that fits in shared memory -- 32 or 16
    rows per J^T W J tile, per-curve statistics in shared memory or in the
    scratch slab -- on a one-wave, three-iteration sample of the group's own
-   items and keeps the fastest (cached per group shape for the process;
-   setting mode 1 clears the cache); mode 0 takes the first layout that fits
-   in that order.  Results do not depend on the layout. */
+   items and keeps the fastest (cached per group shape for the process);
+   mode 2 is mode 1 with the cache cleared first; mode 0 takes the first
+   layout that fits in that order.  Results do not depend on the layout. */
 ps_status ps_batch_set_tuning(int32_t mode);
 /* JSON description of the last ps_gpu_scan_batch's groups: padded
    coefficient count, objects, resident CTAs, candidate layouts with their

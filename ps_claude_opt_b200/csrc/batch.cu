@@ -529,10 +529,10 @@ extern "C" ps_status ps_gpu_scan_batch(int32_t device, int32_t n_obj, const ps_o
 
 extern "C" ps_status ps_batch_set_tuning(int32_t mode)
 {
-    if (mode != 0 && mode != 1) return psb_fail(PS_ERR_ARG, "ps_batch_set_tuning: mode must be 0 or 1");
+    if (mode < 0 || mode > 2) return psb_fail(PS_ERR_ARG, "ps_batch_set_tuning: mode must be 0, 1 or 2");
     std::lock_guard<std::mutex> lk(tuning().mu);
-    tuning().mode = mode;
-    if (mode == 1) tuning().cache.clear();
+    tuning().mode = mode == 0 ? 0 : 1;
+    if (mode == 2) tuning().cache.clear();
     return PS_OK;
 }
 

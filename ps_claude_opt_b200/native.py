@@ -430,7 +430,8 @@ def scan_batch(objs, device=0, quirks=0, max_freq=None):
 
 
 def batch_set_tuning(mode):
-    """ps_batch_set_tuning: 1 = autotuned tile layouts (default), 0 = the
+    """ps_batch_set_tuning: 1 = autotuned tile layouts (default; choices
+    cached per group shape), 2 = the same after clearing the cache, 0 = the
     first layout that fits."""
     _check(lib().ps_batch_set_tuning(int(mode)))
 
