@@ -65,11 +65,13 @@ def build(quiet: bool = True) -> None:
 _LIBS: dict = {}
 
 
-def lib(fast: bool = False, fma: bool = False) -> C.CDLL:
+def lib(fast: bool = False, fma: bool = False, perturb: bool = False) -> C.CDLL:
     """The strict oracle; fast=True the -O3 -march=native build (timed CPU
     baseline); fma=True the build with FMA contraction (the same algorithm
-    under a different rounding)."""
-    name = "libps_oracle_fma.so" if fma else ("libps_oracle_fast.so" if fast else "libps_oracle.so")
+    under a different rounding); perturb=True the strict build with the
+    seeded brightness noise of oracle/perturbation_study.py."""
+    name = ("libps_oracle_perturb.so" if perturb else "libps_oracle_fma.so" if fma else
+            "libps_oracle_fast.so" if fast else "libps_oracle.so")
     if name not in _LIBS:
         path = os.path.join(BUILD, name)
         if not os.path.exists(path):
@@ -215,11 +217,12 @@ class OracleModel:
                           threads or os.cpu_count() or 1)
         return float(cw[0]), int(nc[0])
 
-    def scan(self, freq_start, freq_end, freq_step, n_start=1, max_lines=None, threads=0, fast=False):
+    def scan(self, freq_start, freq_end, freq_step, n_start=1, max_lines=None, threads=0, fast=False,
+             perturb=False):
         n_max = int((freq_start - freq_end) / freq_step) + 1
         cap = n_max - n_start + 1 if max_lines is None else max_lines
         lines = (Line * max(cap, 1))()
-        n = lib(fast).pso_scan(C.byref(self.m), freq_start, freq_end, freq_step, n_start, lines, cap,
+        n = lib(fast, perturb=perturb).pso_scan(C.byref(self.m), freq_start, freq_end, freq_step, n_start, lines, cap,
                                threads or os.cpu_count() or 1)
         return np.array([(l.period_h, l.rms, l.chisq, l.dark, l.lambda_deg, l.beta_deg)
                          for l in lines[:n]])

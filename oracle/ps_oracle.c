@@ -418,6 +418,28 @@ static double shape_areas(const pso_model *m, const double *a, double *area)
 /* Brightness and derivative row of one point: mrqcof_curve1_opt
    (Start.cu:2262-2535), one point at a time.  row[p-1] = d ymod / d a_p
    (un-renormalised); returns ymod = br * scale. */
+#ifdef PSO_PERTURB
+/* Perturbation study (test infrastructure, built only as
+   _build/libps_oracle_perturb.so): every brightness term of an evaluation
+   made during LM iteration < PSO_PERTURB_UNTIL is multiplied by
+   1 + PSO_PERTURB_EPS * u, u uniform in [-1, 1] from a hash of (fit,
+   iteration, point, term), to measure how much relative error the
+   50-iteration fits tolerate before they end elsewhere. */
+#include <stdint.h>
+static __thread int g_iter = 0;
+static __thread uint64_t g_fit = 0;
+static double perturb_eps(void) { const char *e = getenv("PSO_PERTURB_EPS"); return e ? atof(e) : 0.0; }
+static int perturb_until(void) { const char *e = getenv("PSO_PERTURB_UNTIL"); return e ? atoi(e) : 1000; }
+static double perturb_u(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    x ^= x >> 31;
+    return (double)(x >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+#endif
+
 static double point_row(const pso_model *m, const double *a, const double *area, int ip,
                         double *row, double *dsh)
 {
@@ -457,6 +479,19 @@ static double point_row(const pso_model *m, const double *a, const double *area,
         }
     }
     double sc = g.scale;
+#ifdef PSO_PERTURB
+    double eps = perturb_eps();
+    if (eps > 0 && g_iter < perturb_until()) {
+        uint64_t base = (g_fit * 1000003ull + (uint64_t)g_iter) * 65537ull + (uint64_t)ip * 131ull;
+        for (int k = 0; k < nc; k++) dsh[k] *= 1.0 + eps * perturb_u(base + k);
+        br *= 1.0 + eps * perturb_u(base + 900);
+        t1 *= 1.0 + eps * perturb_u(base + 901);
+        t2 *= 1.0 + eps * perturb_u(base + 902);
+        t3 *= 1.0 + eps * perturb_u(base + 903);
+        t4 *= 1.0 + eps * perturb_u(base + 904);
+        t5 *= 1.0 + eps * perturb_u(base + 905);
+    }
+#endif
     for (int k = 0; k < nc; k++) row[k] = sc * dsh[k];
     row[nc + 0] = sc * t1;
     row[nc + 1] = sc * t2;
@@ -681,6 +716,9 @@ void pso_fit(const pso_model *m, double freq_start, double freq_step, int n_freq
     double a[PSO_MAX_PAR + 1], atry[PSO_MAX_PAR + 1];
     memset(atry, 0, sizeof(atry));
     initial_params(m, freq_start, freq_step, n_freq, pole, a);
+#ifdef PSO_PERTURB
+    g_fit = (uint64_t)n_freq * 16 + (uint64_t)pole;
+#endif
 
     double alamda = -1, chisq = 0, ochisq = 0;
     int niter = 0, status = 0;
@@ -690,6 +728,9 @@ void pso_fit(const pso_model *m, double freq_start, double freq_step, int n_freq
     for (;;) {
         int go = ((niter < m->n_iter_max) && (iter_diff > m->iter_diff_max)) || (niter < m->n_iter_min);
         if (!go) break;
+#ifdef PSO_PERTURB
+        g_iter = niter;
+#endif
         int first = 0;
         if (alamda < 0) {
             alamda = m->alamda_start;
