@@ -567,13 +567,16 @@ def main():
            + it.nbytes)
     d2h = n_fits * rec
     e2e_ms = []
-    for s in range(max(1, min(args.steps, 3))):
+    e2e_clocks = ClockSampler(local_rank)
+    e2e_clocks.start()
+    for s in range(max(1, min(args.steps, 5))):
         flush.fill_(s)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         eng.configure(conw_r=obj.conw_r)
         eng.fit_items(it[:, 0], it[:, 1])
         e2e_ms.append((time.perf_counter() - t0) * 1000)
+    e2e_clk = e2e_clocks.stop()
     e2e_value = n_fits * world / (np.mean(e2e_ms) / 1000.0)
 
     # the same steps with the mixed-precision sweep (FP32 facet terms, 3xTF32
@@ -619,7 +622,8 @@ def main():
                          "flops_per_launch": fl, "mean_niter": niter},
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "ms_per_step": float(np.mean(e2e_ms))},
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": float(np.mean(e2e_ms)),
+                    "ms_per_step_each": [float(v) for v in e2e_ms], "clocks": e2e_clk},
             "gpu_launches": args.steps,
             "mixed": {"value": mixed_value, "unit": "fits/s", "ms_per_step": mixed_ms / args.steps,
                       "s_per_object": n_obj / (mixed_value / world), "gpu_launches": args.steps,
