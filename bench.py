@@ -661,13 +661,15 @@ def main():
         screened_s = time.perf_counter() - t0
         b = screen.best_line(lines)
         sm = {"s_per_object": screened_s, "ranking_s": t_rank, "fitted_frequencies": int(len(idx)),
-              "first_selection": plan.initial, "edge_expansions": plan.expansions, "fallback": plan.fallback,
+              "first_selection": plan.initial, "edge_expansions": plan.expansions,
+              "period_doubling_probes": plan.alias_probes, "fallback": plan.fallback,
               "fallback_reason": plan.reason, "n_frequencies": int(n_max), "fits": int(10 * len(idx)),
               "vs_plain_fp64_full_scan_s": n_max * 10 / value,
               "speedup_vs_plain_fp64_full_scan": (n_max * 10 / value) / screened_s,
               "best_frequency": int(idx[b]),
               "note": "top 3.4 % of the network's ranking with one neighbour each side plus a 2 % random audit, "
-                      "widened around a best line at a run edge, full grid if the audit contradicts the ranking; "
+                      "widened around a best line at a run edge, its period-doubling partners probed, full grid "
+                      "if the audit contradicts the ranking; "
                       "mixed-precision fits; trained network ps_claude_opt_b200/screen_model.bin"}
         if fix:
             got = native.format_lines(lines[b:b + 1]).strip()

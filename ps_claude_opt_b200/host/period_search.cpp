@@ -30,7 +30,8 @@
 //     --screen MODEL fit only the frequencies a trained screening network
 //                    ranks first (the top 3.4 % with one neighbour on either
 //                    side, plus a 2 % audit sample), widen around a best line
-//                    at the edge of a fitted run, and fall back to the whole
+//                    at the edge of a fitted run, probe its period-doubling
+//                    partners, and fall back to the whole
 //                    grid when the audit sample contradicts the ranking; one
 //                    output line per fitted frequency, in frequency order; no
 //                    checkpoints
@@ -225,7 +226,9 @@ void screen_parts(const std::vector<float> &score, double top, int halo, double 
 // Control flow of a screened scan (ps_claude_opt_b200.screen.plan_scan):
 // fit the core and the audit sample; while the best line has an unfitted
 // neighbour, fit kEdge more frequencies each side of it (at most
-// kMaxExpansions times, then fall back); if an audit frequency farther than
+// kMaxExpansions times, then fall back); fit the neighbourhoods of the best
+// line's period-doubling partners (twice and half its frequency) once per
+// best line, widening again if one wins; if an audit frequency farther than
 // kEdge from the best line comes within kAuditMargin (relative) of its rms,
 // fall back.  Falling back fits every remaining frequency, which makes the
 // output the full scan's.
@@ -236,7 +239,7 @@ constexpr int kMaxExpansions = 8;
 struct ScreenedScan {
     std::vector<ps_line> line;   // per frequency (valid where fitted)
     std::vector<char> fitted;
-    int initial = 0, expansions = 0;
+    int initial = 0, expansions = 0, alias_probes = 0;
     bool fallback = false;
     const char *reason = "";
 };
@@ -402,22 +405,38 @@ int main(int argc, char **argv)
         for (int f = 0; f < n_last; ++f) first[f] = core[f] || aud[f];
         bool ok = fit(0, n_last - 1, &first);
         for (int f = 0; f < n_last; ++f) sc.initial += sc.fitted[f];
-        while (ok) {
+        std::vector<char> probed(n_last, 0);
+        while (ok && !sc.fallback) {
+            // widen around a best line at the edge of a fitted run
+            while (ok) {
+                const int b = best_fitted(sc);
+                if (b < 0) {
+                    sc.fallback = true;
+                    sc.reason = "edge";
+                    break;
+                }
+                const bool open = (b > 0 && !sc.fitted[b - 1]) || (b + 1 < n_last && !sc.fitted[b + 1]);
+                if (!open) break;
+                if (sc.expansions >= kMaxExpansions) {
+                    sc.fallback = true;
+                    sc.reason = "edge";
+                    break;
+                }
+                ok = fit(b - kEdge, b + kEdge, nullptr);
+                ++sc.expansions;
+            }
+            if (!ok || sc.fallback) break;
+            // probe the best line's period-doubling partners (twice and half its frequency) once
             const int b = best_fitted(sc);
-            if (b < 0) {
-                sc.fallback = true;
-                sc.reason = "edge";
-                break;
+            if (probed[b]) break;
+            probed[b] = 1;
+            const double fb = obj.freq_start - b * obj.freq_step;
+            for (double t : {2.0 * fb, 0.5 * fb}) {
+                const int a = (int)std::lround((obj.freq_start - t) / obj.freq_step);
+                if (ok && a >= 0 && a < n_last) ok = fit(a - kEdge, a + kEdge, nullptr);
             }
-            const bool open = (b > 0 && !sc.fitted[b - 1]) || (b + 1 < n_last && !sc.fitted[b + 1]);
-            if (!open) break;
-            if (sc.expansions >= kMaxExpansions) {
-                sc.fallback = true;
-                sc.reason = "edge";
-                break;
-            }
-            ok = fit(b - kEdge, b + kEdge, nullptr);
-            ++sc.expansions;
+            ++sc.alias_probes;
+            if (best_fitted(sc) == b) break;
         }
         if (ok && !sc.fallback) {
             const int b = best_fitted(sc);
@@ -443,9 +462,9 @@ int main(int argc, char **argv)
         std::fclose(out);
         std::fprintf(stderr,
                      "period_search: screened scan fitted %d of %d frequencies (first selection %d, %d edge "
-                     "expansions%s%s)\n",
-                     n_fit, n_last, sc.initial, sc.expansions, sc.fallback ? ", fell back to the full grid: " : "",
-                     sc.reason);
+                     "expansions, %d period-doubling probes%s%s)\n",
+                     n_fit, n_last, sc.initial, sc.expansions, sc.alias_probes,
+                     sc.fallback ? ", fell back to the full grid: " : "", sc.reason);
         ps_gpu_unprepare(h);
         return 0;
     }

@@ -248,6 +248,7 @@ class Plan:
         self.rms = {}            # frequency -> best rms over the poles (NaN kept)
         self.initial = 0         # frequencies of the first selection
         self.expansions = 0      # edge expansions
+        self.alias_probes = 0    # best lines whose period-doubling partners were fitted
         self.fallback = False    # the whole grid was fitted
         self.reason = ""         # why it fell back: "audit" or "edge"
 
@@ -265,8 +266,22 @@ class Plan:
         return b
 
 
+def alias_indices(freqs, b):
+    """0-based grid indices nearest the period-doubling partners of frequency
+    index b (twice and half its frequency) that lie on the grid."""
+    f0, df = float(freqs[0]), float(freqs[0] - freqs[1]) if len(freqs) > 1 else 0.0
+    if df <= 0:
+        return []
+    out = []
+    for t in (2.0 * freqs[b], 0.5 * freqs[b]):
+        i = int(round((f0 - t) / df))
+        if 0 <= i < len(freqs):
+            out.append(i)
+    return out
+
+
 def plan_scan(pred, fit, top=0.034, halo=1, audit=0.02, seed=0, margin=AUDIT_MARGIN, edge=EDGE_WIDTH,
-              max_expansions=MAX_EXPANSIONS):
+              max_expansions=MAX_EXPANSIONS, freqs=None):
     """The screened scan's control flow, independent of the device.
 
     fit(indices) fits the given 0-based frequencies (all poles) and returns
@@ -275,11 +290,17 @@ def plan_scan(pred, fit, top=0.034, halo=1, audit=0.02, seed=0, margin=AUDIT_MAR
       2. while the best line sits at the edge of a fitted run (a neighbour is
          unfitted), fit `edge` more frequencies on each side of it -- at most
          `max_expansions` times, then fall back;
-      3. judge by the audit sample: if an audit frequency away from the best
+      3. with the grid's frequencies given (freqs), fit the neighbourhoods
+         (+-edge) of the best line's period-doubling partners, twice and half
+         its frequency -- a double-peaked lightcurve fits almost as well at
+         twice its period, so the ranking can put the wrong one of the pair
+         first -- and return to step 2 if one of them wins; each best line is
+         probed once;
+      4. judge by the audit sample: if an audit frequency away from the best
          line's neighbourhood comes within `margin` (relative) of the best
          rms, the network's ranking is not trustworthy for this object and
          the scan falls back;
-      4. on fallback, fit every remaining frequency: the result is then the
+      5. on fallback, fit every remaining frequency: the result is then the
          full scan's.
     Returns a Plan."""
     n = len(pred)
@@ -294,19 +315,34 @@ def plan_scan(pred, fit, top=0.034, halo=1, audit=0.02, seed=0, margin=AUDIT_MAR
 
     run(core | aud)
     plan.initial = len(plan.rms)
-    while True:
+    probed = set()
+    while not plan.fallback:
+        while True:
+            b = plan.best()
+            if b < 0:
+                plan.fallback, plan.reason = True, "edge"
+                break
+            need = [j for j in (b - 1, b + 1) if 0 <= j < n and j not in plan.rms]
+            if not need:
+                break
+            if plan.expansions >= max_expansions:
+                plan.fallback, plan.reason = True, "edge"
+                break
+            run(range(b - edge, b + edge + 1))
+            plan.expansions += 1
+        if plan.fallback or freqs is None:
+            break
         b = plan.best()
-        if b < 0:
-            plan.fallback, plan.reason = True, "edge"
+        if b in probed:
             break
-        need = [j for j in (b - 1, b + 1) if 0 <= j < n and j not in plan.rms]
-        if not need:
+        probed.add(b)
+        around = set()
+        for a in alias_indices(freqs, b):
+            around.update(range(a - edge, a + edge + 1))
+        run(around)
+        plan.alias_probes += 1
+        if plan.best() == b:
             break
-        if plan.expansions >= max_expansions:
-            plan.fallback, plan.reason = True, "edge"
-            break
-        run(range(b - edge, b + edge + 1))
-        plan.expansions += 1
     if not plan.fallback:
         b = plan.best()
         br = plan.rms[b]
@@ -338,8 +374,9 @@ def screened_scan(obj, net, conw_r, top=0.034, halo=1, audit=0.02, seed=0, devic
                   precision=native.PRECISION_FP64, margin=AUDIT_MARGIN, pred=None):
     """Fits the screened frequencies (after the convexity-weight search,
     whose conw_r is passed in), expanding around a best line at the edge of
-    a fitted run and falling back to the whole grid when the audit sample
-    contradicts the ranking (plan_scan).  Returns (frequency indices
+    a fitted run, probing its period-doubling partners and falling back to
+    the whole grid when the audit sample contradicts the ranking
+    (plan_scan).  Returns (frequency indices
     1-based, lines, per-fit results [n, 10, 6], Plan)."""
     if pred is None:
         pred = net.predict(normalise(features(obj, frequencies(obj), device)))
@@ -358,7 +395,7 @@ def screened_scan(obj, net, conw_r, top=0.034, halo=1, audit=0.02, seed=0, devic
                 store[q] = (res[i], lines[i])
             return lines[:, 1]
 
-        plan = plan_scan(pred, fit, top, halo, audit, seed, margin)
+        plan = plan_scan(pred, fit, top, halo, audit, seed, margin, freqs=frequencies(obj))
     idx = np.array(plan.fitted, dtype=np.int64)
     res = np.stack([store[i][0] for i in idx])
     lines = np.stack([store[i][1] for i in idx])

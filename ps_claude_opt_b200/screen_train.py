@@ -173,17 +173,48 @@ def judge(net, fulls, top=0.034, halo=1, audit=0.02, log=print, precision=native
     return hits, rows
 
 
+def _hit(full_best, full_fields, idx, lines, bs):
+    """The screened best line (lines[bs] at frequency idx[bs]) is the full
+    scan's: same frequency, or period within 0.1 h, rms within 0.1 and pole
+    within 1 degree (full_fields: the full scan's printed best line, split)."""
+    sb = lines[bs]
+    fp, fr, fl, fbeta = float(full_fields[0]), float(full_fields[1]), float(full_fields[4]), float(full_fields[5])
+    dl = abs((fl - sb[4] + 180.0) % 360.0 - 180.0)
+    return bool(idx[bs] == full_best or (abs(fp - sb[0]) < 0.1 and abs(fr - sb[1]) < 0.1 and dl < 1.0 and
+                                         abs(fbeta - sb[5]) < 1.0))
+
+
+def screen_row(net, i, obj, truth, n_freq, conw_r, full_best, full_line, t_full, precision=native.PRECISION_MIXED):
+    """One held-out object's screened scans -- in `precision` (the screened
+    + mixed form by default) and in FP64, which separates the ranking's
+    misses from lines that only the precision moved -- judged against the
+    full FP64 scan's best line (1-based frequency, printed line)."""
+    full_fields = full_line.split()
+    t0 = time.time()
+    idx, lines, _, plan = screen.screened_scan(obj, net, conw_r, seed=i, precision=precision)
+    t_scr = time.time() - t0
+    bs = screen.best_line(lines)
+    idx64, lines64, _, plan64 = screen.screened_scan(obj, net, conw_r, seed=i, precision=native.PRECISION_FP64)
+    bs64 = screen.best_line(lines64)
+    return dict(seed=EVAL_SEED + i, n_freq=n_freq, conw_r=conw_r, full_best=full_best, full_line=full_line,
+                screened_best=int(idx[bs]), screened_line=native.format_lines(lines[bs:bs + 1]).strip(),
+                ok=_hit(full_best, full_fields, idx, lines, bs), same_frequency=bool(idx[bs] == full_best),
+                ok_fp64_screen=_hit(full_best, full_fields, idx64, lines64, bs64),
+                fp64_screen_best=int(idx64[bs64]), fp64_screen_fallback=plan64.fallback,
+                fp64_screen_fitted=int(len(idx64)), fitted=int(len(idx)), initial=plan.initial,
+                expansions=plan.expansions, alias_probes=plan.alias_probes, fallback=plan.fallback,
+                reason=plan.reason, full_s_per_object=t_full, screened_s=t_scr,
+                true_period_h=float(truth["period_h"]), precision=int(precision))
+
+
 def judge_stream(net, start, count, out_path, precision=native.PRECISION_MIXED, group=8, log=print):
     """The held-out judgement at scale, one JSON line per object appended to
     out_path as soon as its group is done (a partial run keeps its rows).
     The judge is the plain FP64 full scan of object EVAL_SEED + start + i
     (convexity-weight search, then all 5000 frequencies x 10 poles), run
     `group` objects at a time through ps_gpu_scan_batch, whose lines are
-    bit-identical to one object at a time; the screened scan runs in
-    `precision` (mixed by default: the screened + mixed form) with its plan
-    (edge expansions, fallback) and the judge's convexity weight.  A hit:
-    the screened best line is the full scan's -- same frequency, or period
-    within 0.1 h, rms within 0.1 and pole within 1 degree."""
+    bit-identical to one object at a time; the screened scans (screen_row)
+    use the judge's convexity weight."""
     done = set()
     try:
         with open(out_path) as f:
@@ -198,24 +229,37 @@ def judge_stream(net, start, count, out_path, precision=native.PRECISION_MIXED, 
         fulls = native.scan_batch([o for o, _ in objs])
         t_full = (time.time() - t0) / len(ids)
         for i, (obj, truth), (full, conw_r) in zip(ids, objs, fulls):
-            t0 = time.time()
-            idx, lines, _, plan = screen.screened_scan(obj, net, conw_r, seed=i, precision=precision)
-            t_scr = time.time() - t0
-            bf, bs = screen.best_line(full), screen.best_line(lines)
-            fb, sb = full[bf], lines[bs]
-            dl = abs((fb[4] - sb[4] + 180.0) % 360.0 - 180.0)
-            ok = bool(idx[bs] == bf + 1 or (abs(fb[0] - sb[0]) < 0.1 and abs(fb[1] - sb[1]) < 0.1 and dl < 1.0 and
-                                            abs(fb[5] - sb[5]) < 1.0))
-            row = dict(seed=EVAL_SEED + i, n_freq=len(full), conw_r=conw_r, full_best=bf + 1,
-                       full_line=native.format_lines(full[bf:bf + 1]).strip(), screened_best=int(idx[bs]),
-                       screened_line=native.format_lines(lines[bs:bs + 1]).strip(), ok=ok,
-                       same_frequency=bool(idx[bs] == bf + 1), fitted=int(len(idx)), initial=plan.initial,
-                       expansions=plan.expansions, fallback=plan.fallback, reason=plan.reason,
-                       full_s_per_object=t_full, screened_s=t_scr, true_period_h=float(truth["period_h"]),
-                       precision=int(precision))
+            bf = screen.best_line(full)
+            row = screen_row(net, i, obj, truth, len(full), conw_r, bf + 1,
+                             native.format_lines(full[bf:bf + 1]).strip(), t_full, precision)
             with open(out_path, "a") as f:
                 f.write(json.dumps(row) + "\n")
             log(json.dumps(row))
+
+
+def rescreen(net, rows_in, out_path, precision=native.PRECISION_MIXED, log=print):
+    """Re-judges the screened scans of objects whose full FP64 scans a
+    judge_stream run already made (its rows: best frequency, printed best
+    line, convexity weight), with the current screen, without scanning them
+    again."""
+    done = set()
+    try:
+        with open(out_path) as f:
+            done = {json.loads(l)["seed"] for l in f if l.strip()}
+    except FileNotFoundError:
+        pass
+    for l in open(rows_in):
+        if not l.strip():
+            continue
+        r = json.loads(l)
+        if r["seed"] in done:
+            continue
+        obj, truth = make_object(r["seed"])
+        row = screen_row(net, r["seed"] - EVAL_SEED, obj, truth, r["n_freq"], r["conw_r"], r["full_best"],
+                         r["full_line"], r["full_s_per_object"], precision)
+        with open(out_path, "a") as f:
+            f.write(json.dumps(row) + "\n")
+        log(json.dumps(row))
 
 
 def main():
@@ -231,11 +275,16 @@ def main():
     ap.add_argument("--model", default=None, help="judge this trained network instead of training one")
     ap.add_argument("--out", default=None)
     ap.add_argument("--judge-out", default=None,
-                    help="stream the held-out judgement (mixed-precision judge) to this JSON-lines file")
+                    help="stream the held-out judgement (FP64 full scans as the judge) to this JSON-lines file")
+    ap.add_argument("--rescreen", default=None,
+                    help="with --judge-out: re-judge the screened scans of the objects in this rows file")
     args = ap.parse_args()
     if args.judge_out:
         net = screen.load_model(args.model or screen.MODEL_PATH)
-        judge_stream(net, args.eval_start, args.eval_objects, args.judge_out)
+        if args.rescreen:
+            rescreen(net, args.rescreen, args.judge_out)
+        else:
+            judge_stream(net, args.eval_start, args.eval_objects, args.judge_out)
         return
     t0 = time.time()
     if args.model:

@@ -155,3 +155,25 @@ def test_plan_falls_back_after_too_many_expansions():
     plan, _ = _plan(pred, rms, top=0.002, halo=0, audit=0.002, max_expansions=3)
     assert plan.fallback and plan.reason in ("edge", "audit") and len(plan.fitted) == n
     assert plan.best() == n - 1
+
+
+def test_plan_probes_the_period_doubling_partner():
+    """A double-peaked curve fits almost as well at twice its period: the
+    ranking puts the doubled period first, the probe of the best line's
+    partners (twice and half its frequency) finds the true one."""
+    from ps_claude_opt_b200 import screen
+
+    n = 2000
+    freqs = 0.30 - 1e-4 * np.arange(n)          # 1/h, decreasing like the reference's grid
+    true_i = 400                                  # f = 0.26
+    alias_i = int(round((0.30 - 0.13) / 1e-4))    # half the frequency: the doubled period
+    rms = _landscape(n, best=true_i, depth=0.3)
+    rms[alias_i] = rms[true_i] * 1.05
+    pred = np.full(n, 5.0)
+    pred[alias_i - 1:alias_i + 2] = -5.0          # the network ranks only the alias first
+    plan, _ = _plan(pred, rms, top=0.0015, halo=1, audit=0.0005, freqs=freqs)
+    assert plan.alias_probes >= 1 and plan.best() == true_i and not plan.fallback
+    assert len(plan.fitted) < 0.02 * n
+    # without the grid the probe is off and the alias stays the answer
+    plan0, _ = _plan(pred, rms, top=0.0015, halo=1, audit=0.0005)
+    assert plan0.best() == alias_i and plan0.alias_probes == 0
