@@ -1,9 +1,10 @@
 """The trained screening network on held-out production-size objects (not in
 its training set): fitting about a tenth of the trial frequencies, the
-screened scan finds the full scan's best line -- same frequency, same line --
-on every object, which an equally large random choice of frequencies (the
-method without the network) does not.  The full-scan best lines come from
-tests/golden/screen_heldout.json (tests/golden/make_screen_fixture.py)."""
+screened scan finds the full scan's best line -- same frequency, same
+printed line -- which an equally large random choice of frequencies (the
+method without the network) mostly does not.  The full-scan best lines come
+from tests/golden/screen_heldout.json (tests/golden/make_screen_fixture.py,
+from the held-out judgement's plain FP64 full scans)."""
 import json
 import os
 
@@ -13,6 +14,12 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "screen_heldout.json")
+
+
+def _printed(lines, b):
+    from ps_claude_opt_b200 import native
+
+    return native.format_lines(lines[b:b + 1]).strip()
 
 
 def test_screen_finds_the_full_scan_best_line_with_a_tenth_of_the_fits():
@@ -32,12 +39,12 @@ def test_screen_finds_the_full_scan_best_line_with_a_tenth_of_the_fits():
         b = screen.best_line(lines)
         if idx[b] == row["best_freq"]:
             net_hits += 1
-            assert np.allclose(lines[b], row["best_line"], rtol=1e-9, atol=1e-9)
+            assert _printed(lines, b) == row["best_line_printed"]   # FP64 fits are deterministic
         rng = np.random.default_rng(row["seed"])
         rand = rng.choice(row["n_freq"], size=len(idx), replace=False) + 1
         random_hits += int(row["best_freq"] in rand)
     assert net_hits == len(rows)
-    assert random_hits < net_hits
+    assert random_hits < net_hits // 2
 
 
 def test_screened_scan_in_mixed_precision_finds_the_same_line():
@@ -49,7 +56,8 @@ def test_screened_scan_in_mixed_precision_finds_the_same_line():
                                             precision=native.PRECISION_MIXED)
     b = screen.best_line(lines)
     assert idx[b] == row["best_freq"]
-    assert abs(lines[b, 0] - row["best_line"][0]) < 1e-4 and abs(lines[b, 1] - row["best_line"][1]) < 1e-4
+    ref = row["best_line_printed"].split()
+    assert abs(lines[b, 0] - float(ref[0])) < 1e-4 and abs(lines[b, 1] - float(ref[1])) < 1e-4
 
 
 def test_rank_through_the_c_abi_matches_the_python_network():
@@ -77,6 +85,8 @@ def _lines(path):
 
 
 def test_host_program_screened_scan_finds_the_best_line(tmp_path):
+    """The host program's --screen (its own convexity-weight search, then
+    the screened scan) prints the full scan's best line."""
     import subprocess
 
     from ps_claude_opt_b200 import native, screen
@@ -87,11 +97,11 @@ def test_host_program_screened_scan_finds_the_best_line(tmp_path):
                        text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     lines = _lines(tmp_path / "period_search_out")
-    assert len(lines) <= 0.125 * row["n_freq"]
+    assert len(lines) <= 0.13 * row["n_freq"]
     b = int(np.argmin(lines[:, 1]))
-    assert abs(lines[b, 0] - row["best_line"][0]) < 1e-6           # period [h], as printed
-    assert abs(lines[b, 1] - row["best_line"][1]) < 1e-6           # rms
-    assert abs(lines[b, 4] - round(row["best_line"][4])) <= 1 and abs(lines[b, 5] - round(row["best_line"][5])) <= 1
+    ref = [float(v) for v in row["best_line_printed"].split()]
+    assert abs(lines[b, 0] - ref[0]) < 1e-6 and abs(lines[b, 1] - ref[1]) < 1e-6   # period [h], rms as printed
+    assert lines[b, 4] == ref[4] and lines[b, 5] == ref[5]
 
 
 def test_host_program_mixed_precision_scan(tmp_path):
