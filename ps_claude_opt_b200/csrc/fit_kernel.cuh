@@ -56,9 +56,11 @@ constexpr int kWS = 12;  // row stride (floats) of the mixed-precision weight ti
 
 // Facets per basis chunk: keeps kStages chunks within ~60 KB of shared memory.
 __host__ __device__ inline int chunk_facets(int ncp) { return ncp <= 64 ? 32 : 16; }
+constexpr int kMaxChunkGroups = 8;  // 4-facet groups per basis chunk, at most
 
 struct Sh {
     double4 *F;       // [n_fac] normal + current area
+    float4 *cone;     // [ceil(n_fac / 4)] per 4-facet group: unit axis, sine of the half-angle + margin
     double *alpha;    // [mfit][ld]
     double *covar;    // [mfit][ld]
     double *beta;     // [kMaxFit]
@@ -196,6 +198,7 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, int 
         return base ? (void *)(base + o) : nullptr;
     };
     void *F = take(sizeof(double4) * n_fac);
+    void *cone = take(sizeof(float4) * ((n_fac + 3) / 4));
     void *alpha = take(sizeof(double) * mfit * ld);
     void *covar = take(sizeof(double) * mfit * ld);
     void *beta = take(sizeof(double) * kMaxFit);
@@ -232,7 +235,7 @@ __host__ __device__ inline size_t carve_bytes(int n_fac, int mfit, int ncp, int 
     void *f32 = take(mixed ? sizeof(float4) * n_fac : 0);
     void *g32 = take(mixed ? sizeof(float2) * n_fac : 0);
     if (s) {
-        s->F = (double4 *)F; s->alpha = (double *)alpha; s->covar = (double *)covar;
+        s->F = (double4 *)F; s->cone = (float4 *)cone; s->alpha = (double *)alpha; s->covar = (double *)covar;
         s->beta = (double *)beta; s->da = (double *)da; s->a = (double *)a; s->atry = (double *)atry;
         s->T = (double *)un;
         s->TW = (double *)(un + tsz);
@@ -302,6 +305,40 @@ static __device__ double shape_areas(const DevObject &o, const Sh &s, const doub
     double v[1] = {part};
     block_sum<1>(v, s.red);
     return v[0];
+}
+
+// Bounding cone of each group of 4 consecutive facets (the facet sweep's
+// step): axis c = normalised sum of the normals, half-angle t = the largest
+// angle between c and a normal.  A unit normal n within t of c has
+// n.e <= cos(angle(c, e) - t), so c.e <= -sin t rules out n.e > 0 for every
+// facet of the group; the sweep skips a group when that holds for every lane
+// and for e or e0.  The sine is stored with a margin of 1e-5 that covers the
+// FP32 rounding of the test (|error| < 1e-6 for unit vectors); a group wider
+// than a hemisphere always passes.  Reads the object's facet table.
+static __device__ void facet_cones(const DevObject &o, const Sh &s)
+{
+    const int ng = (o.n_fac + 3) >> 2;
+    for (int g = threadIdx.x; g < ng; g += kThreads) {
+        const int f0 = 4 * g, nq = min(4, o.n_fac - f0);
+        double4 n[4];
+        double cx = 0, cy = 0, cz = 0;
+        for (int q = 0; q < nq; ++q) {
+            n[q] = ldg4(&o.facet[f0 + q]);
+            cx += n[q].x; cy += n[q].y; cz += n[q].z;
+        }
+        const double len = sqrt(cx * cx + cy * cy + cz * cz);
+        float4 c = make_float4(1.f, 0.f, 0.f, 2.f);  // degenerate: always passes
+        if (len > 1e-3) {
+            cx /= len; cy /= len; cz /= len;
+            double cmin = 1.0;
+            for (int q = 0; q < nq; ++q) cmin = fmin(cmin, n[q].x * cx + n[q].y * cy + n[q].z * cz);
+            if (cmin > 0.0) {
+                const double sn = sqrt(fmax(0.0, 1.0 - cmin * cmin));
+                c = make_float4((float)cx, (float)cy, (float)cz, (float)(sn + 1e-5));
+            }
+        }
+        s.cone[g] = c;
+    }
 }
 
 // Per-evaluation invariants from a: phase function, scattering weights and the
@@ -491,10 +528,18 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
 // MMAs (m8n8k4), A = w (8 points x 4 facets, staged through a per-warp
 // shared-memory tile), B = the basis chunk (4 facets x 8 coefficients),
 // accumulators [4 point blocks][ncp / 8 coefficient blocks] in registers.
-template <int NCP>
+//
+// When the last coefficient block holds a single coefficient (n_coef = 8k + 1:
+// every lmax = mmax model with lmax even, e.g. 25, 49, 81 coefficients), that
+// coefficient runs on the FP64 FMA pipe instead (lane = point, four FMAs per
+// step) and the block's MMAs are skipped: they would spend 8 columns of tensor
+// work on one.  The lane's accumulator is element C[0][NT - 1][0], which the
+// skipped MMAs leave free.
+template <int NCP, bool X1>
 __device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows, const int *perm)
 {
     constexpr int NT = NCP / 8;
+    constexpr int NTM = X1 ? NT - 1 : NT;  // coefficient blocks on the tensor cores
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int np = o.n_points, nf = o.n_fac, nc = o.n_coef;
     const double cl = s.inv[5], cls = s.inv[6];
@@ -541,6 +586,80 @@ __device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows, c
             for (int n = 0; n < NT; ++n) C[m][n][0] = C[m][n][1] = 0.0;
         double br = 0, u0 = 0, u1 = 0, u2 = 0, w0 = 0, w1 = 0, w2 = 0, t4 = 0, t5 = 0;
 
+        // Lambert + Lommel-Seeliger terms of facets k0..k0+3 of the chunk for
+        // this lane's point: the rotation sums, the brightness and the facet
+        // weights wk (the MMA's A operand); with X1 also the single last
+        // coefficient.  Lanes that do not see a facet run the same arithmetic
+        // on finite stand-ins and contribute exact zeros.
+        auto facet_terms = [&](int f0, int nfc, const double *yb, int k0, double (&wk)[4]) {
+            double4 fr[4];
+            double mu[4], mu0[4];
+            bool vis[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const bool inside = k0 + q < nfc;
+                fr[q] = s.F[f0 + (inside ? k0 + q : 0)];
+                mu[q] = ex * fr[q].x + ey * fr[q].y + ez * fr[q].z;
+                mu0[q] = sx * fr[q].x + sy * fr[q].y + sz * fr[q].z;
+                vis[q] = act && inside && (mu[q] > kTiny) && (mu0[q] > kTiny);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double ar = vis[q] ? fr[q].w : 0.0;
+                const double r = rcp_nr(vis[q] ? mu[q] + mu0[q] : 1.0);
+                const double sv = mu[q] * mu0[q] * (cl + cls * r);
+                const double q0 = mu0[q] * r, q1 = mu[q] * r;
+                const double dsmu = cls * (q0 * q0) + cl * mu0[q];
+                const double dsmu0 = cls * (q1 * q1) + cl * mu[q];
+                const double amm = ar * mu[q] * mu0[q];
+                const double w = ar * sv;
+                const double gg = ar * dsmu;
+                const double g0 = ar * dsmu0;
+                br += w;
+                u0 = fma(gg, fr[q].x, u0);
+                u1 = fma(gg, fr[q].y, u1);
+                u2 = fma(gg, fr[q].z, u2);
+                w0 = fma(g0, fr[q].x, w0);
+                w1 = fma(g0, fr[q].y, w1);
+                w2 = fma(g0, fr[q].z, w2);
+                t4 += amm;
+                t5 += amm * r;
+                wk[q] = w;
+            }
+            if constexpr (X1) {
+                // the single last coefficient, lane = point
+                const double *yl = yb + (size_t)k0 * NCP + 8 * (NT - 1);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const double y = (k0 + q < nfc) ? yl[(size_t)q * NCP] : 0.0;
+                    C[0][NT - 1][0] = fma(wk[q], y, C[0][NT - 1][0]);
+                }
+            }
+        };
+        // The weights of one group through the warp's shared-memory tile into
+        // the m8n8k4 A fragments: a[m] = w[point 8m + lane/4][facet lane%4].
+        auto stage = [&](const double (&wk)[4], double (&a)[4]) {
+            __syncwarp();  // every lane has read the previous group's tile
+            reinterpret_cast<double2 *>(wt)[2 * lane] = make_double2(wk[0], wk[1]);
+            reinterpret_cast<double2 *>(wt)[2 * lane + 1] = make_double2(wk[2], wk[3]);
+            __syncwarp();
+#pragma unroll
+            for (int m = 0; m < 4; ++m) a[m] = wt[(8 * m + (lane >> 2)) * 4 + (lane & 3)];
+        };
+        // One k-step of the shape-derivative GEMM: facets kp..kp+3 of the chunk.
+        auto mma_step = [&](const double *yb, int nfc, int kp, const double (&a)[4]) {
+            // B row = facet kp + (lane & 3); rows past the chunk's end hold
+            // stale data and must contribute zeros
+            const bool brow = kp + (lane & 3) < nfc;
+            const double *yr = yb + (size_t)(kp + (lane & 3)) * NCP + (lane >> 2);
+#pragma unroll
+            for (int n = 0; n < NTM; ++n) {
+                const double bv = brow ? yr[8 * n] : 0.0;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) dmma_8x8x4(C[m][n][0], C[m][n][1], a[m], bv);
+            }
+        };
+
         for (int c = 0; c < nchunks; ++c, ++g) {
             const int b = g % kStages;
             const int use = s.ctl[C_YUSE + b] + g / kStages;  // phase parity of this fill
@@ -548,71 +667,47 @@ __device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows, c
             if (tile_act) {
                 const int f0 = c * fc, nfc = min(fc, nf - f0);
                 const double *yb = s.ybuf + (size_t)b * fc * NCP;
+                // the chunk's 4-facet groups that some lane may see: a bounding-cone
+                // test per group in FP32 (necessary for visibility, see facet_cones);
+                // the groups it rules out would add exact zeros
+                unsigned gmask = 0;
+                if (act) {
+                    const float ex32 = (float)ex, ey32 = (float)ey, ez32 = (float)ez;
+                    const float sx32 = (float)sx, sy32 = (float)sy, sz32 = (float)sz;
+                    const float4 *cg = s.cone + (f0 >> 2);
+#pragma unroll
+                    for (int q = 0; q < kMaxChunkGroups; ++q) {
+                        if (4 * q < nfc) {
+                            const float4 cn = cg[q];
+                            const float ce = fmaf(ez32, cn.z, fmaf(ey32, cn.y, ex32 * cn.x));
+                            const float c0 = fmaf(sz32, cn.z, fmaf(sy32, cn.y, sx32 * cn.x));
+                            if (ce > -cn.w && c0 > -cn.w) gmask |= 1u << q;
+                        }
+                    }
+                }
+                gmask = __reduce_or_sync(0xffffffffu, gmask);
+                // Software pipeline over the chunk's groups: the facet terms of
+                // group k0 and the tensor-core step of the group before it (A
+                // fragments already in registers) form one branch-free stretch, so
+                // each warp always has FP64 FMA and MMA work ready to interleave.
+                // Groups the cone test passes but no lane sees add exact zeros.
+                if (gmask) {
+                    double a[4], wk[4];
+                    int k0 = 4 * (__ffs(gmask) - 1);
+                    gmask &= gmask - 1;
+                    facet_terms(f0, nfc, yb, k0, wk);
+                    stage(wk, a);
+                    int kp = k0;
 #pragma unroll 1
-                for (int k0 = 0; k0 < nfc; k0 += 4) {
-                    // four facets per step: visibility first, one vote, then four
-                    // independent branch-free chains the scheduler can interleave
-                    double4 fr[4];
-                    double mu[4], mu0[4];
-                    bool vis[4];
-                    bool v4 = false;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const bool inside = k0 + q < nfc;
-                        fr[q] = s.F[f0 + (inside ? k0 + q : 0)];
-                        mu[q] = ex * fr[q].x + ey * fr[q].y + ez * fr[q].z;
-                        mu0[q] = sx * fr[q].x + sy * fr[q].y + sz * fr[q].z;
-                        vis[q] = act && inside && (mu[q] > kTiny) && (mu0[q] > kTiny);
-                        v4 = v4 || vis[q];
+                    while (gmask) {
+                        k0 = 4 * (__ffs(gmask) - 1);
+                        gmask &= gmask - 1;
+                        facet_terms(f0, nfc, yb, k0, wk);
+                        mma_step(yb, nfc, kp, a);
+                        stage(wk, a);
+                        kp = k0;
                     }
-                    const bool any4 = __any_sync(0xffffffffu, v4);
-                    double wk[4] = {0.0, 0.0, 0.0, 0.0};
-                    if (any4) {
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            // lanes that do not see the facet run the same arithmetic on
-                            // finite stand-ins and contribute exact zeros
-                            const double ar = vis[q] ? fr[q].w : 0.0;
-                            const double r = rcp_nr(vis[q] ? mu[q] + mu0[q] : 1.0);
-                            const double sv = mu[q] * mu0[q] * (cl + cls * r);
-                            const double q0 = mu0[q] * r, q1 = mu[q] * r;
-                            const double dsmu = cls * (q0 * q0) + cl * mu0[q];
-                            const double dsmu0 = cls * (q1 * q1) + cl * mu[q];
-                            const double amm = ar * mu[q] * mu0[q];
-                            const double w = ar * sv;
-                            const double gg = ar * dsmu;
-                            const double g0 = ar * dsmu0;
-                            br += w;
-                            u0 = fma(gg, fr[q].x, u0);
-                            u1 = fma(gg, fr[q].y, u1);
-                            u2 = fma(gg, fr[q].z, u2);
-                            w0 = fma(g0, fr[q].x, w0);
-                            w1 = fma(g0, fr[q].y, w1);
-                            w2 = fma(g0, fr[q].z, w2);
-                            t4 += amm;
-                            t5 += amm * r;
-                            wk[q] = w;
-                        }
-                    }
-                    if (any4) {  // warp-uniform
-                        reinterpret_cast<double2 *>(wt)[2 * lane] = make_double2(wk[0], wk[1]);
-                        reinterpret_cast<double2 *>(wt)[2 * lane + 1] = make_double2(wk[2], wk[3]);
-                        __syncwarp();
-                        double a[4];
-#pragma unroll
-                        for (int m = 0; m < 4; ++m) a[m] = wt[(8 * m + (lane >> 2)) * 4 + (lane & 3)];
-                        // B row = facet k0 + (lane & 3); rows past the chunk's end hold
-                        // stale data and must contribute zeros
-                        const bool brow = k0 + (lane & 3) < nfc;
-                        const double *yr = yb + (size_t)(k0 + (lane & 3)) * NCP + (lane >> 2);
-#pragma unroll
-                        for (int n = 0; n < NT; ++n) {
-                            const double bv = brow ? yr[8 * n] : 0.0;
-#pragma unroll
-                            for (int m = 0; m < 4; ++m) dmma_8x8x4(C[m][n][0], C[m][n][1], a[m], bv);
-                        }
-                        __syncwarp();
-                    }
+                    mma_step(yb, nfc, kp, a);
                 }
             }
             // release the buffer; the last of the kWarps warps refills it
@@ -640,6 +735,7 @@ __device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows, c
             const double scale = geo.scale;
             if (act) {
                 double *row = rows + (size_t)p * o.row_stride;
+                if constexpr (X1) row[nc - 1] = scale * C[0][NT - 1][0];
                 row[nc + 0] = scale * t1;
                 row[nc + 1] = scale * t2;
                 row[nc + 2] = scale * t3;
@@ -662,6 +758,7 @@ __device__ void brightness_rows(const DevObject &o, const Sh &s, double *rows, c
                 double *row = rows + (size_t)pm * o.row_stride;
 #pragma unroll
                 for (int n = 0; n < NT; ++n) {
+                    if (n >= NTM) break;
                     const int k = 8 * n + 2 * (lane & 3);
                     if (k + 1 < nc)
                         *reinterpret_cast<double2 *>(row + k) = make_double2(sm * C[m][n][0], sm * C[m][n][1]);
@@ -1127,7 +1224,10 @@ __device__ double evaluate(const DevObject &o, const DevParams &p, const Sh &s, 
     if constexpr (MIXED)
         brightness_rows_mixed<NCP>(o, s, rows, perm);
     else
-        brightness_rows<NCP>(o, s, rows, perm);
+        if (o.n_coef == NCP - 7)
+            brightness_rows<NCP, true>(o, s, rows, perm);
+        else
+            brightness_rows<NCP, false>(o, s, rows, perm);
     // the tile phase reads the rows back through the bulk-copy (async) proxy
     asm volatile("fence.proxy.async.global;" ::: "memory");
     __syncthreads();
@@ -1881,6 +1981,7 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
 
     if constexpr (!BATCH) {
         for (int f = tid; f < o.n_fac; f += kThreads) s.F[f] = ldg4(&o.facet[f]);
+        facet_cones(o, s);
         if (tid < o.mfit) s.fidx[tid] = __ldg(&o.fidx[tid]);
     }
     if (tid == 0) {
@@ -1937,6 +2038,7 @@ fit_kernel(DevObject o, DevParams p, const FitItem *items, int n_items, int *que
                 }
                 __syncthreads();
                 for (int f = tid; f < s_obj.n_fac; f += kThreads) s.F[f] = ldg4(&s_obj.facet[f]);
+                facet_cones(s_obj, s);
                 if (tid < s_obj.mfit) s.fidx[tid] = __ldg(&s_obj.fidx[tid]);
                 __syncthreads();
                 cur = k;
