@@ -262,6 +262,41 @@ def rescreen(net, rows_in, out_path, precision=native.PRECISION_MIXED, log=print
         log(json.dumps(row))
 
 
+def summarize(rows):
+    """Totals of held-out judgement rows (judge_stream / rescreen output), one
+    row per object: hits of the screened + mixed scan and of the screened
+    FP64 scan against the FP64 full scan's best line, the one-sided 95 %
+    lower bound of the hit rate (Clopper-Pearson), fallbacks to the full
+    grid, frequencies fitted, and the period ratio of each miss to the full
+    scan's best period (2 or 1/2: a period-doubling alias)."""
+    from scipy.stats import beta as beta_dist
+
+    n = len(rows)
+    if n == 0:
+        return dict(objects=0)
+    hits = sum(bool(r["ok"]) for r in rows)
+    hits64 = sum(bool(r.get("ok_fp64_screen", r["ok"])) for r in rows)
+    lower = float(beta_dist.ppf(0.05, hits, n - hits + 1)) if hits > 0 else 0.0
+    misses = []
+    for r in rows:
+        if r["ok"]:
+            continue
+        full_p = float(r["full_line"].split()[0])
+        scr_p = float(r["screened_line"].split()[0]) if r.get("screened_line") else float("nan")
+        misses.append(dict(seed=r["seed"], full_period_h=full_p, screened_period_h=scr_p,
+                           ratio=scr_p / full_p if full_p else float("nan")))
+    fitted = np.array([r["fitted"] for r in rows], dtype=float)
+    return dict(objects=n, hits=hits, hit_rate=hits / n, hit_rate_lower95=lower, hits_fp64_screen=hits64,
+                fallbacks=sum(bool(r["fallback"]) for r in rows),
+                expansions=int(sum(int(r.get("expansions", 0)) for r in rows)),
+                alias_probes=int(sum(int(r.get("alias_probes", 0)) for r in rows)),
+                fitted_mean=float(fitted.mean()), fitted_max=int(fitted.max()),
+                n_freq=int(rows[0]["n_freq"]),
+                screened_s_mean=float(np.mean([r["screened_s"] for r in rows])),
+                full_s_mean=float(np.mean([r["full_s_per_object"] for r in rows])),
+                misses=misses)
+
+
 def main():
     import os
 
@@ -278,7 +313,13 @@ def main():
                     help="stream the held-out judgement (FP64 full scans as the judge) to this JSON-lines file")
     ap.add_argument("--rescreen", default=None,
                     help="with --judge-out: re-judge the screened scans of the objects in this rows file")
+    ap.add_argument("--summarize", nargs="+", default=None,
+                    help="print the totals of these judgement rows files (no GPU work)")
     args = ap.parse_args()
+    if args.summarize:
+        rows = [json.loads(l) for path in args.summarize for l in open(path) if l.strip()]
+        print(json.dumps(summarize(rows), indent=1))
+        return
     if args.judge_out:
         net = screen.load_model(args.model or screen.MODEL_PATH)
         if args.rescreen:

@@ -177,3 +177,29 @@ def test_plan_probes_the_period_doubling_partner():
     # without the grid the probe is off and the alias stays the answer
     plan0, _ = _plan(pred, rms, top=0.0015, halo=1, audit=0.0005)
     assert plan0.best() == alias_i and plan0.alias_probes == 0
+
+
+def test_judgement_summary_counts_hits_fallbacks_and_aliases():
+    """screen_train.summarize on hand-made judgement rows: hit rate with its
+    one-sided 95 % Clopper-Pearson lower bound, fallbacks, and the period
+    ratio of a miss (2.0: the screened scan ended at twice the period)."""
+    from ps_claude_opt_b200 import screen_train
+
+    def row(seed, ok, scr_p=10.0, fallback=False, fitted=520):
+        return dict(seed=seed, ok=ok, ok_fp64_screen=ok, fallback=fallback, fitted=fitted, n_freq=5000,
+                    expansions=1, alias_probes=2, screened_s=2.0, full_s_per_object=26.0,
+                    full_line="10.00000000  0.020000  1.000000  1.0  100   20",
+                    screened_line="%.8f  0.020000  1.000000  1.0  100   20" % scr_p)
+
+    rows = [row(i, True) for i in range(9)] + [row(9, False, scr_p=20.0, fallback=True, fitted=5000)]
+    s = screen_train.summarize(rows)
+    assert s["objects"] == 10 and s["hits"] == 9 and s["fallbacks"] == 1
+    assert abs(s["hit_rate"] - 0.9) < 1e-12
+    # Clopper-Pearson: 9 of 10 -> P(X >= 9 | p) = 0.05 at p = 0.6058
+    assert abs(s["hit_rate_lower95"] - 0.6058) < 1e-3
+    assert s["fitted_max"] == 5000 and abs(s["fitted_mean"] - (9 * 520 + 5000) / 10) < 1e-9
+    assert len(s["misses"]) == 1 and abs(s["misses"][0]["ratio"] - 2.0) < 1e-12
+    assert screen_train.summarize([]) == {"objects": 0}
+    # all hits: 200 of 200 -> lower bound 0.05 ** (1 / 200)
+    s = screen_train.summarize([row(i, True) for i in range(200)])
+    assert abs(s["hit_rate_lower95"] - 0.05 ** (1 / 200)) < 1e-9
