@@ -663,20 +663,23 @@ def main():
         sm = {"s_per_object": screened_s, "ranking_s": t_rank, "fitted_frequencies": int(len(idx)),
               "first_selection": plan.initial, "edge_expansions": plan.expansions,
               "period_doubling_probes": plan.alias_probes, "fallback": plan.fallback,
-              "fallback_reason": plan.reason, "n_frequencies": int(n_max), "fits": int(10 * len(idx)),
+              "fallback_reason": plan.reason, "n_frequencies": int(n_max),
+              "fits": int(10 * (len(idx) + plan.polished)), "fp64_refitted_frequencies": plan.polished,
               "vs_plain_fp64_full_scan_s": n_max * 10 / value,
               "speedup_vs_plain_fp64_full_scan": (n_max * 10 / value) / screened_s,
               "best_frequency": int(idx[b]),
               "note": "top 3.4 % of the network's ranking with one neighbour each side plus a 2 % random audit, "
                       "widened around a best line at a run edge, its period-doubling partners probed, full grid "
                       "if the audit contradicts the ranking; "
-                      "mixed-precision fits; trained network ps_claude_opt_b200/screen_model.bin"}
+                      "mixed-precision fits, then the candidate lines (best line, its period-doubling partners, "
+                      "the lowest local minima) refitted in FP64; trained network ps_claude_opt_b200/screen_model.bin"}
         if fix:
             got = native.format_lines(lines[b:b + 1]).strip()
             sm["best_line_matches_full"] = bool(int(idx[b]) == fix["best_freq"] and
                                                 got.split()[3:] == fix["formatted_best"].split()[3:] and
                                                 abs(lines[b, 0] - fix["best_line"][0]) < 0.1 and
                                                 abs(lines[b, 1] - fix["best_line"][1]) < 0.1)
+            sm["best_line_printed_equal"] = got == fix["formatted_best"]
             sm["best_line"] = got
             sm["full_scan_best_line"] = fix["formatted_best"]
         line["screened_mixed"] = sm

@@ -235,14 +235,64 @@ void screen_parts(const std::vector<float> &score, double top, int halo, double 
 constexpr double kAuditMargin = 0.10;
 constexpr int kEdge = 2;
 constexpr int kMaxExpansions = 8;
+// Mixed precision: the candidates are refitted in FP64
+// (ps_claude_opt_b200.screen.polish_plan): in the first round the
+// kPolishMinima lowest local minima of the rms (an unfitted or NaN neighbour
+// counts as higher) with one neighbour each side; in every round the best
+// line and its period-doubling partners with kEdge neighbours each side;
+// rounds repeat while they add frequencies, at most kPolishRounds times.
+constexpr int kPolishMinima = 8;
+constexpr int kPolishRounds = 4;
 
 struct ScreenedScan {
     std::vector<ps_line> line;   // per frequency (valid where fitted)
     std::vector<char> fitted;
-    int initial = 0, expansions = 0, alias_probes = 0;
+    int initial = 0, expansions = 0, alias_probes = 0, polished = 0;
     bool fallback = false;
     const char *reason = "";
 };
+
+// 0-based grid indices nearest the period-doubling partners (twice and half
+// the frequency) of index b that lie on the grid of n frequencies.
+std::vector<int> alias_indices(double freq_start, double freq_step, int n, int b)
+{
+    std::vector<int> out;
+    if (freq_step <= 0) return out;
+    const double fb = freq_start - b * freq_step;
+    for (double t : {2.0 * fb, 0.5 * fb}) {
+        const int a = (int)std::lround((freq_start - t) / freq_step);
+        if (a >= 0 && a < n) out.push_back(a);
+    }
+    return out;
+}
+
+// The frequencies one polish round refits: sorted, on the grid, not yet done.
+std::vector<int> polish_set(const ScreenedScan &sc, double freq_start, double freq_step, int b, bool first,
+                            const std::vector<char> &done)
+{
+    const int n = (int)sc.line.size();
+    std::vector<char> need(n, 0);
+    auto mark = [&](int lo, int hi) {
+        for (int i = std::max(0, lo); i <= std::min(n - 1, hi); ++i) need[i] = 1;
+    };
+    mark(b - kEdge, b + kEdge);
+    for (int a : alias_indices(freq_start, freq_step, n, b)) mark(a - kEdge, a + kEdge);
+    if (first) {
+        auto key = [&](int i) {
+            if (i < 0 || i >= n || !sc.fitted[i] || std::isnan(sc.line[i].rms)) return (double)INFINITY;
+            return sc.line[i].rms;
+        };
+        std::vector<int> loc;
+        for (int i = 0; i < n; ++i)
+            if (key(i) < INFINITY && key(i) <= key(i - 1) && key(i) <= key(i + 1)) loc.push_back(i);
+        std::stable_sort(loc.begin(), loc.end(), [&](int x, int y) { return key(x) < key(y); });
+        for (size_t q = 0; q < loc.size() && q < (size_t)kPolishMinima; ++q) mark(loc[q] - 1, loc[q] + 1);
+    }
+    std::vector<int> out;
+    for (int i = 0; i < n; ++i)
+        if (need[i] && !done[i]) out.push_back(i);
+    return out;
+}
 
 int best_fitted(const ScreenedScan &sc)
 {
@@ -374,11 +424,8 @@ int main(int argc, char **argv)
         ScreenedScan sc;
         sc.line.resize(n_last);
         sc.fitted.assign(n_last, 0);
-        // fits the unfitted frequencies among [lo, hi] whose mask is set
-        auto fit = [&](int lo, int hi, const std::vector<char> *mask) {
-            std::vector<int> sel;
-            for (int f = std::max(0, lo); f <= std::min(n_last - 1, hi); ++f)
-                if (!sc.fitted[f] && (!mask || (*mask)[f])) sel.push_back(f);
+        // fits (or refits) the given frequencies, all poles, and keeps their lines
+        auto fit_list = [&](const std::vector<int> &sel) {
             if (sel.empty()) return true;
             std::vector<int32_t> nf, pl;
             for (int f : sel)
@@ -400,6 +447,13 @@ int main(int argc, char **argv)
                 sc.fitted[f] = 1;
             }
             return true;
+        };
+        // fits the unfitted frequencies among [lo, hi] whose mask is set
+        auto fit = [&](int lo, int hi, const std::vector<char> *mask) {
+            std::vector<int> sel;
+            for (int f = std::max(0, lo); f <= std::min(n_last - 1, hi); ++f)
+                if (!sc.fitted[f] && (!mask || (*mask)[f])) sel.push_back(f);
+            return fit_list(sel);
         };
         std::vector<char> first(n_last);
         for (int f = 0; f < n_last; ++f) first[f] = core[f] || aud[f];
@@ -430,11 +484,8 @@ int main(int argc, char **argv)
             const int b = best_fitted(sc);
             if (probed[b]) break;
             probed[b] = 1;
-            const double fb = obj.freq_start - b * obj.freq_step;
-            for (double t : {2.0 * fb, 0.5 * fb}) {
-                const int a = (int)std::lround((obj.freq_start - t) / obj.freq_step);
-                if (ok && a >= 0 && a < n_last) ok = fit(a - kEdge, a + kEdge, nullptr);
-            }
+            for (int a : alias_indices(obj.freq_start, obj.freq_step, n_last, b))
+                if (ok) ok = fit(a - kEdge, a + kEdge, nullptr);
             ++sc.alias_probes;
             if (best_fitted(sc) == b) break;
         }
@@ -448,6 +499,23 @@ int main(int argc, char **argv)
                 }
         }
         if (ok && sc.fallback) ok = fit(0, n_last - 1, nullptr);
+        if (ok && opt.precision == PS_PRECISION_MIXED) {
+            // the candidates' final fits in FP64
+            ok = ps_gpu_set_precision(h, PS_PRECISION_FP64) == PS_OK &&
+                 ps_gpu_configure(h, obj.freq_start, obj.freq_step, obj.stop_condition, obj.n_iter_min, conw_r,
+                                  conw_r, obj.n_points, obj.ia.data(), ia_par, obj.cg_first.data(), obj.sig.data(),
+                                  obj.sigr2.data(), obj.n_fac, obj.brightness.data(), &curves, &shape) == PS_OK;
+            std::vector<char> done(n_last, 0);
+            for (int round = 0; ok && round < kPolishRounds; ++round) {
+                const int b = best_fitted(sc);
+                if (b < 0) break;
+                const std::vector<int> sel = polish_set(sc, obj.freq_start, obj.freq_step, b, round == 0, done);
+                if (sel.empty()) break;
+                ok = fit_list(sel);
+                for (int f : sel) done[f] = 1;
+                sc.polished += (int)sel.size();
+            }
+        }
         if (!ok) {
             std::fclose(out);
             ps_gpu_unprepare(h);
@@ -462,9 +530,9 @@ int main(int argc, char **argv)
         std::fclose(out);
         std::fprintf(stderr,
                      "period_search: screened scan fitted %d of %d frequencies (first selection %d, %d edge "
-                     "expansions, %d period-doubling probes%s%s)\n",
+                     "expansions, %d period-doubling probes%s%s; %d refitted in FP64)\n",
                      n_fit, n_last, sc.initial, sc.expansions, sc.alias_probes,
-                     sc.fallback ? ", fell back to the full grid: " : "", sc.reason);
+                     sc.fallback ? ", fell back to the full grid: " : "", sc.reason, sc.polished);
         ps_gpu_unprepare(h);
         return 0;
     }

@@ -206,6 +206,8 @@ def _lcg_uniform(seed, n):
 AUDIT_MARGIN = 0.10     # an audit line within 10 % of the screened best rms (the validator's rms envelope)
 EDGE_WIDTH = 2          # frequencies fitted on each side of a best line that sits at the edge of a fitted run
 MAX_EXPANSIONS = 8      # edge expansions before the scan falls back to the full grid
+POLISH_MINIMA = 8       # mixed-precision scans: lowest local minima refitted in FP64 (with +-1 neighbours)
+POLISH_ROUNDS = 4       # ... and at most this many rounds of FP64 refits around a moving best line
 
 
 def select_parts(pred, top=0.034, halo=1, audit=0.02, seed=0):
@@ -251,6 +253,8 @@ class Plan:
         self.alias_probes = 0    # best lines whose period-doubling partners were fitted
         self.fallback = False    # the whole grid was fitted
         self.reason = ""         # why it fell back: "audit" or "edge"
+        self.polished = 0        # mixed precision: frequencies refitted in FP64
+        self.polish_rounds = 0
 
     @property
     def fitted(self):
@@ -355,6 +359,52 @@ def plan_scan(pred, fit, top=0.034, halo=1, audit=0.02, seed=0, margin=AUDIT_MAR
     return plan
 
 
+def polish_plan(plan, fit64, freqs, edge=EDGE_WIDTH, minima=POLISH_MINIMA, rounds=POLISH_ROUNDS):
+    """FP64 decision for a scan whose fits ran in mixed precision.
+
+    FP32 facet sums move a fit's rms at the 1e-3 level, enough to reorder
+    two nearly equal minima -- most often a period and its double, which a
+    double-peaked lightcurve fits almost equally well.  So the candidates
+    are refitted in FP64 (fit64(indices) returns their best rms, and the
+    caller replaces their lines): in the first round the `minima` lowest
+    local minima of the rms over the fitted frequencies (an unfitted or NaN
+    neighbour counts as higher) with one neighbour on either side; in every
+    round the best line with `edge` neighbours on either side and the same
+    neighbourhoods of its period-doubling partners (twice and half its
+    frequency).  Rounds repeat while they add frequencies -- the best line
+    can move to a refitted one -- at most `rounds` times.  Refitted
+    frequencies may include ones the screen had not fitted; they become
+    fitted lines.  Updates plan.rms, plan.polished, plan.polish_rounds."""
+    n = plan.n
+    done = set()
+
+    def key(i):
+        r = plan.rms.get(i, np.inf)
+        return np.inf if np.isnan(r) else r
+
+    for rnd in range(rounds):
+        b = plan.best()
+        if b < 0:
+            break
+        need = set(range(b - edge, b + edge + 1))
+        for a in alias_indices(freqs, b):
+            need.update(range(a - edge, a + edge + 1))
+        if rnd == 0:
+            loc = [i for i in plan.fitted if key(i) < np.inf and key(i) <= key(i - 1) and key(i) <= key(i + 1)]
+            loc.sort(key=lambda i: (key(i), i))
+            for i in loc[:minima]:
+                need.update((i - 1, i, i + 1))
+        need = sorted(i for i in need if 0 <= i < n and i not in done)
+        if not need:
+            break
+        for i, r in zip(need, fit64(np.array(need, dtype=np.int64))):
+            plan.rms[i] = float(r)
+        done.update(need)
+        plan.polished = len(done)
+        plan.polish_rounds = rnd + 1
+    return plan
+
+
 def _best_pole_lines(obj, idx, res):
     """One line per frequency from the 10 poles' results, as the reference
     prints it (start_CUDA.cu:1200-1229): NaN-safe, the earliest pole wins ties."""
@@ -371,12 +421,13 @@ def _best_pole_lines(obj, idx, res):
 
 
 def screened_scan(obj, net, conw_r, top=0.034, halo=1, audit=0.02, seed=0, device=0,
-                  precision=native.PRECISION_FP64, margin=AUDIT_MARGIN, pred=None):
+                  precision=native.PRECISION_FP64, margin=AUDIT_MARGIN, pred=None, polish=True):
     """Fits the screened frequencies (after the convexity-weight search,
     whose conw_r is passed in), expanding around a best line at the edge of
     a fitted run, probing its period-doubling partners and falling back to
     the whole grid when the audit sample contradicts the ranking
-    (plan_scan).  Returns (frequency indices
+    (plan_scan); in mixed precision the candidate lines are then refitted
+    in FP64 (polish_plan; polish=False leaves them mixed).  Returns (frequency indices
     1-based, lines, per-fit results [n, 10, 6], Plan)."""
     if pred is None:
         pred = net.predict(normalise(features(obj, frequencies(obj), device)))
@@ -396,6 +447,11 @@ def screened_scan(obj, net, conw_r, top=0.034, halo=1, audit=0.02, seed=0, devic
             return lines[:, 1]
 
         plan = plan_scan(pred, fit, top, halo, audit, seed, margin, freqs=frequencies(obj))
+        if precision == native.PRECISION_MIXED and polish:
+            # the candidates' final fits in FP64 (polish_plan)
+            eng.set_precision(native.PRECISION_FP64)
+            eng.configure(conw_r=conw_r)
+            polish_plan(plan, fit, frequencies(obj))
     idx = np.array(plan.fitted, dtype=np.int64)
     res = np.stack([store[i][0] for i in idx])
     lines = np.stack([store[i][1] for i in idx])

@@ -184,26 +184,37 @@ def _hit(full_best, full_fields, idx, lines, bs):
                                          abs(fbeta - sb[5]) < 1.0))
 
 
-def screen_row(net, i, obj, truth, n_freq, conw_r, full_best, full_line, t_full, precision=native.PRECISION_MIXED):
+FP64_SCREEN_FIELDS = ("ok_fp64_screen", "fp64_screen_best", "fp64_screen_fallback", "fp64_screen_fitted")
+
+
+def screen_row(net, i, obj, truth, n_freq, conw_r, full_best, full_line, t_full, precision=native.PRECISION_MIXED,
+               fp64_row=None):
     """One held-out object's screened scans -- in `precision` (the screened
     + mixed form by default) and in FP64, which separates the ranking's
     misses from lines that only the precision moved -- judged against the
-    full FP64 scan's best line (1-based frequency, printed line)."""
+    full FP64 scan's best line (1-based frequency, printed line).  fp64_row:
+    an earlier row of the same object whose FP64 screened-scan fields are
+    reused instead of running that scan again (its inputs are unchanged)."""
     full_fields = full_line.split()
     t0 = time.time()
     idx, lines, _, plan = screen.screened_scan(obj, net, conw_r, seed=i, precision=precision)
     t_scr = time.time() - t0
     bs = screen.best_line(lines)
-    idx64, lines64, _, plan64 = screen.screened_scan(obj, net, conw_r, seed=i, precision=native.PRECISION_FP64)
-    bs64 = screen.best_line(lines64)
+    if fp64_row is not None:
+        fp64 = {k: fp64_row[k] for k in FP64_SCREEN_FIELDS}
+    else:
+        idx64, lines64, _, plan64 = screen.screened_scan(obj, net, conw_r, seed=i, precision=native.PRECISION_FP64)
+        bs64 = screen.best_line(lines64)
+        fp64 = dict(ok_fp64_screen=_hit(full_best, full_fields, idx64, lines64, bs64),
+                    fp64_screen_best=int(idx64[bs64]), fp64_screen_fallback=plan64.fallback,
+                    fp64_screen_fitted=int(len(idx64)))
     return dict(seed=EVAL_SEED + i, n_freq=n_freq, conw_r=conw_r, full_best=full_best, full_line=full_line,
                 screened_best=int(idx[bs]), screened_line=native.format_lines(lines[bs:bs + 1]).strip(),
                 ok=_hit(full_best, full_fields, idx, lines, bs), same_frequency=bool(idx[bs] == full_best),
-                ok_fp64_screen=_hit(full_best, full_fields, idx64, lines64, bs64),
-                fp64_screen_best=int(idx64[bs64]), fp64_screen_fallback=plan64.fallback,
-                fp64_screen_fitted=int(len(idx64)), fitted=int(len(idx)), initial=plan.initial,
+                **fp64, fitted=int(len(idx)), initial=plan.initial,
                 expansions=plan.expansions, alias_probes=plan.alias_probes, fallback=plan.fallback,
-                reason=plan.reason, full_s_per_object=t_full, screened_s=t_scr,
+                reason=plan.reason, polished=plan.polished, polish_rounds=plan.polish_rounds,
+                full_s_per_object=t_full, screened_s=t_scr,
                 true_period_h=float(truth["period_h"]), precision=int(precision))
 
 
@@ -241,7 +252,7 @@ def rescreen(net, rows_in, out_path, precision=native.PRECISION_MIXED, log=print
     """Re-judges the screened scans of objects whose full FP64 scans a
     judge_stream run already made (its rows: best frequency, printed best
     line, convexity weight), with the current screen, without scanning them
-    again."""
+    again; rows that carry the FP64 screened scan's fields keep them."""
     done = set()
     try:
         with open(out_path) as f:
@@ -255,8 +266,9 @@ def rescreen(net, rows_in, out_path, precision=native.PRECISION_MIXED, log=print
         if r["seed"] in done:
             continue
         obj, truth = make_object(r["seed"])
+        reuse = r if all(k in r for k in FP64_SCREEN_FIELDS) else None
         row = screen_row(net, r["seed"] - EVAL_SEED, obj, truth, r["n_freq"], r["conw_r"], r["full_best"],
-                         r["full_line"], r["full_s_per_object"], precision)
+                         r["full_line"], r["full_s_per_object"], precision, fp64_row=reuse)
         with open(out_path, "a") as f:
             f.write(json.dumps(row) + "\n")
         log(json.dumps(row))

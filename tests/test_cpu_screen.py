@@ -203,3 +203,45 @@ def test_judgement_summary_counts_hits_fallbacks_and_aliases():
     # all hits: 200 of 200 -> lower bound 0.05 ** (1 / 200)
     s = screen_train.summarize([row(i, True) for i in range(200)])
     assert abs(s["hit_rate_lower95"] - 0.05 ** (1 / 200)) < 1e-9
+
+
+def test_polish_refits_candidates_and_lets_the_fp64_line_win():
+    """Mixed-precision rms puts the doubled period (the alias) just below
+    the true one; the FP64 refits of the candidates -- the best line, its
+    period-doubling partners, the lowest local minima -- restore the true
+    line, and frequencies outside those neighbourhoods keep their mixed rms."""
+    from ps_claude_opt_b200 import screen
+
+    n = 2000
+    freqs = 0.30 - 1e-4 * np.arange(n)
+    true_i = 400
+    alias_i = int(round((0.30 - 0.13) / 1e-4))
+    rms64 = _landscape(n, best=true_i, depth=0.3)
+    rms64[alias_i] = rms64[true_i] * 1.002                 # FP64: the true line wins
+    rms_mixed = rms64 * (1.0 + 1e-4 * np.cos(np.arange(n)))
+    rms_mixed[alias_i] = rms64[true_i] * 0.999             # mixed: the alias wins
+    pred = np.full(n, 5.0)
+    pred[alias_i - 1:alias_i + 2] = -5.0
+    pred[true_i - 1:true_i + 2] = -4.0
+    plan, _ = _plan(pred, rms_mixed, top=0.003, halo=1, audit=0.0005, freqs=freqs)
+    assert plan.best() == alias_i
+    refits = []
+
+    def fit64(idx):
+        refits.append(idx.tolist())
+        return rms64[idx]
+
+    before = dict(plan.rms)
+    screen.polish_plan(plan, fit64, freqs)
+    assert plan.best() == true_i
+    done = {i for r in refits for i in r}
+    assert {alias_i, true_i} <= done and plan.polished == len(done)
+    assert 1 <= plan.polish_rounds <= screen.POLISH_ROUNDS
+    assert len(done) <= 5 + 10 + 3 * screen.POLISH_MINIMA + 5 * 2 * (screen.POLISH_ROUNDS - 1)
+    for i in set(before) - done:
+        assert plan.rms[i] == before[i]
+    for i in done:
+        assert plan.rms[i] == rms64[i]
+    # a second pass over the polished plan keeps the FP64 best line
+    screen.polish_plan(plan, fit64, freqs)
+    assert plan.best() == true_i

@@ -120,3 +120,58 @@ def test_host_program_mixed_precision_scan(tmp_path):
     assert a.shape == b.shape
     assert np.all(np.abs(a[:, 0] - b[:, 0]) < 0.1) and np.all(np.abs(a[:, 1] - b[:, 1]) < 0.1)
     assert int(np.argmin(a[:, 1])) == int(np.argmin(b[:, 1]))
+
+
+FULLSCANS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "screen_heldout_fullscans.jsonl")
+# held-out objects whose mixed-precision screened scan, without its FP64
+# polish, ended at the period-doubling alias of the full scan's best line
+# (twice and half its period), with a lower mixed-precision rms there
+ALIAS_SEEDS = (8000014, 8000099)
+
+
+def _fullscan(seed):
+    for l in open(FULLSCANS):
+        r = json.loads(l)
+        if r["seed"] == seed:
+            return r
+    raise KeyError(seed)
+
+
+@pytest.mark.parametrize("seed", ALIAS_SEEDS)
+def test_mixed_screen_polish_restores_the_fp64_best_line(seed):
+    """The FP64 refits of the candidates (screen.polish_plan) make the mixed
+    screened scan report the full FP64 scan's best line, printed line for
+    printed line; without them it reports the alias."""
+    from ps_claude_opt_b200 import native, screen, screen_train
+
+    row = _fullscan(seed)
+    obj, _ = screen_train.make_object(seed)
+    net = screen.load_model()
+    idx, lines, _, plan = screen.screened_scan(obj, net, row["conw_r"], precision=native.PRECISION_MIXED)
+    b = screen.best_line(lines)
+    assert idx[b] == row["full_best"] and _printed(lines, b) == row["full_line"]
+    assert 0 < plan.polished <= 5 + 10 + 3 * screen.POLISH_MINIMA + 10 * (screen.POLISH_ROUNDS - 1)
+    idx0, lines0, _, _ = screen.screened_scan(obj, net, row["conw_r"], precision=native.PRECISION_MIXED,
+                                              polish=False)
+    b0 = screen.best_line(lines0)
+    ratio = float(lines0[b0, 0]) / float(row["full_line"].split()[0])
+    assert idx0[b0] != row["full_best"] and min(abs(ratio - 2.0), abs(ratio - 0.5)) < 0.01
+
+
+def test_host_program_mixed_screen_polish(tmp_path):
+    """The host program's --precision mixed --screen takes the same FP64
+    polish and prints the full scan's best line."""
+    import subprocess
+
+    from ps_claude_opt_b200 import native, screen
+
+    row = _fullscan(ALIAS_SEEDS[0])
+    _write_input(tmp_path, row["seed"])
+    r = subprocess.run([native.HOST_PROGRAM, "--precision", "mixed", "--screen", screen.MODEL_PATH], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert "refitted in FP64" in r.stderr
+    text = (tmp_path / "period_search_out").read_text().splitlines()
+    lines = _lines(tmp_path / "period_search_out")
+    b = int(np.argmin(lines[:, 1]))
+    assert text[b].strip() == row["full_line"]
