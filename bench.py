@@ -35,11 +35,11 @@ SEED = 1000003 * 2          # production config, object 0
 FITS_PER_CTA = 10           # fits per resident CTA in one step
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes per fit of the fit kernel on this workload: dram__bytes_read.sum +
-# dram__bytes_write.sum = 12.05 + 14.32 = 26.37 GB over the 148 fits of one
+# dram__bytes_write.sum = 12.41 + 14.32 = 26.73 GB over the 148 fits of one
 # ncu capture of `bench.py --profile-case` (profiles/fit_kernel_production_object.md;
 # the derivative-row scratch round trip, which grows with the number of fits,
 # so a launch's traffic is this times its fits).
-NCU_DRAM_BYTES_PER_FIT = 26.37e9 / 148
+NCU_DRAM_BYTES_PER_FIT = 26.73e9 / 148
 METRIC = ("LM fits/s of the plain FP64 full scan of the production object on 1 B200 (s/object of it and of "
           "the screened+mixed scan in the same line)")
 
