@@ -47,6 +47,7 @@
 
 #include "ps_b200.h"
 #include "ps_input.h"
+#include "screen_flow.h"
 
 namespace {
 
@@ -191,121 +192,6 @@ bool read_model(const std::string &path, std::vector<int32_t> &sizes, std::vecto
     return ok;
 }
 
-// The frequencies (0-based) a screened scan fits first: the core -- the
-// lowest-scoring `top` share with `halo` neighbours each side -- and an
-// `audit` share of the rest drawn by a partial Fisher-Yates shuffle from a
-// 64-bit linear congruential generator (ps_claude_opt_b200.screen.select_parts
-// draws the same sample).  core[i] / audit[i] mark the two sets.
-void screen_parts(const std::vector<float> &score, double top, int halo, double audit, uint64_t seed,
-                  std::vector<char> &core, std::vector<char> &aud)
-{
-    const int n = (int)score.size();
-    std::vector<int> order(n);
-    for (int i = 0; i < n; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return score[a] < score[b]; });
-    const int k = std::max(1, (int)std::nearbyint(top * n));
-    core.assign(n, 0);
-    aud.assign(n, 0);
-    for (int r = 0; r < k; ++r)
-        for (int d = -halo; d <= halo; ++d)
-            if (order[r] + d >= 0 && order[r] + d < n) core[order[r] + d] = 1;
-    std::vector<int> rest;
-    for (int i = 0; i < n; ++i)
-        if (!core[i]) rest.push_back(i);
-    const int na = std::min((int)rest.size(), std::max(1, (int)std::nearbyint(audit * n)));
-    uint64_t x = seed * 2654435761ull + 1ull;
-    for (int j = 0; j < na; ++j) {
-        x = 6364136223846793005ull * x + 1442695040888963407ull;
-        const uint64_t r = x >> 33;
-        const int pick = j + (int)(r % (uint64_t)(rest.size() - j));
-        std::swap(rest[j], rest[pick]);
-        aud[rest[j]] = 1;
-    }
-}
-
-// Control flow of a screened scan (ps_claude_opt_b200.screen.plan_scan):
-// fit the core and the audit sample; while the best line has an unfitted
-// neighbour, fit kEdge more frequencies each side of it (at most
-// kMaxExpansions times, then fall back); fit the neighbourhoods of the best
-// line's period-doubling partners (twice and half its frequency) once per
-// best line, widening again if one wins; if an audit frequency farther than
-// kEdge from the best line comes within kAuditMargin (relative) of its rms,
-// fall back.  Falling back fits every remaining frequency, which makes the
-// output the full scan's.
-constexpr double kAuditMargin = 0.10;
-constexpr int kEdge = 2;
-constexpr int kMaxExpansions = 8;
-// Mixed precision: the candidates are refitted in FP64
-// (ps_claude_opt_b200.screen.polish_plan): in the first round the
-// kPolishMinima lowest local minima of the rms (an unfitted or NaN neighbour
-// counts as higher) with one neighbour each side; in every round the best
-// line and its period-doubling partners with kEdge neighbours each side;
-// rounds repeat while they add frequencies, at most kPolishRounds times.
-constexpr int kPolishMinima = 8;
-constexpr int kPolishRounds = 4;
-
-struct ScreenedScan {
-    std::vector<ps_line> line;   // per frequency (valid where fitted)
-    std::vector<char> fitted;
-    int initial = 0, expansions = 0, alias_probes = 0, polished = 0;
-    bool fallback = false;
-    const char *reason = "";
-};
-
-// 0-based grid indices nearest the period-doubling partners (twice and half
-// the frequency) of index b that lie on the grid of n frequencies.
-std::vector<int> alias_indices(double freq_start, double freq_step, int n, int b)
-{
-    std::vector<int> out;
-    if (freq_step <= 0) return out;
-    const double fb = freq_start - b * freq_step;
-    for (double t : {2.0 * fb, 0.5 * fb}) {
-        const int a = (int)std::lround((freq_start - t) / freq_step);
-        if (a >= 0 && a < n) out.push_back(a);
-    }
-    return out;
-}
-
-// The frequencies one polish round refits: sorted, on the grid, not yet done.
-std::vector<int> polish_set(const ScreenedScan &sc, double freq_start, double freq_step, int b, bool first,
-                            const std::vector<char> &done)
-{
-    const int n = (int)sc.line.size();
-    std::vector<char> need(n, 0);
-    auto mark = [&](int lo, int hi) {
-        for (int i = std::max(0, lo); i <= std::min(n - 1, hi); ++i) need[i] = 1;
-    };
-    mark(b - kEdge, b + kEdge);
-    for (int a : alias_indices(freq_start, freq_step, n, b)) mark(a - kEdge, a + kEdge);
-    if (first) {
-        auto key = [&](int i) {
-            if (i < 0 || i >= n || !sc.fitted[i] || std::isnan(sc.line[i].rms)) return (double)INFINITY;
-            return sc.line[i].rms;
-        };
-        std::vector<int> loc;
-        for (int i = 0; i < n; ++i)
-            if (key(i) < INFINITY && key(i) <= key(i - 1) && key(i) <= key(i + 1)) loc.push_back(i);
-        std::stable_sort(loc.begin(), loc.end(), [&](int x, int y) { return key(x) < key(y); });
-        for (size_t q = 0; q < loc.size() && q < (size_t)kPolishMinima; ++q) mark(loc[q] - 1, loc[q] + 1);
-    }
-    std::vector<int> out;
-    for (int i = 0; i < n; ++i)
-        if (need[i] && !done[i]) out.push_back(i);
-    return out;
-}
-
-int best_fitted(const ScreenedScan &sc)
-{
-    int b = -1;
-    double br = INFINITY;
-    for (size_t i = 0; i < sc.line.size(); ++i)
-        if (sc.fitted[i] && sc.line[i].rms < br) {   // NaN never wins; the first minimum wins ties
-            b = (int)i;
-            br = sc.line[i].rms;
-        }
-    return b;
-}
-
 int fail(const char *what)
 {
     std::fprintf(stderr, "period_search: %s: %s\n", what, ps_last_error());
@@ -413,7 +299,7 @@ int main(int argc, char **argv)
             return fail("screen");
         }
         std::vector<char> core, aud;
-        screen_parts(score, 0.034, 1, 0.02, 0, core, aud);
+        psflow::screen_parts(score, 0.034, 1, 0.02, 0, core, aud);
         if (ps_gpu_configure(h, obj.freq_start, obj.freq_step, obj.stop_condition, obj.n_iter_min, conw_r, conw_r,
                              obj.n_points, obj.ia.data(), ia_par, obj.cg_first.data(), obj.sig.data(),
                              obj.sigr2.data(), obj.n_fac, obj.brightness.data(), &curves, &shape) != PS_OK) {
@@ -421,12 +307,10 @@ int main(int argc, char **argv)
             ps_gpu_unprepare(h);
             return fail("screened scan");
         }
-        ScreenedScan sc;
-        sc.line.resize(n_last);
-        sc.fitted.assign(n_last, 0);
-        // fits (or refits) the given frequencies, all poles, and keeps their lines
-        auto fit_list = [&](const std::vector<int> &sel) {
-            if (sel.empty()) return true;
+        psflow::Plan sc(n_last);
+        std::vector<ps_line> line(n_last);
+        // fits the given frequencies, all poles: keeps their lines, returns their rms
+        auto fit = [&](const std::vector<int> &sel, std::vector<double> &rms) {
             std::vector<int32_t> nf, pl;
             for (int f : sel)
                 for (int p = 0; p < PS_N_POLES; ++p) {
@@ -442,79 +326,20 @@ int main(int argc, char **argv)
                     if (best < 0 || (!std::isnan(r[p].dev) && !(r[p].dev >= r[best].dev))) best = p;
                 const ps_fit_result &b = r[best];
                 const int f = sel[q];
-                sc.line[f] = ps_line{24 * b.per, b.dev, b.dev * b.dev * obj.n_points,
-                                     f == 0 ? conw_r * obj.escl * obj.escl : b.dark, b.lambda_deg, b.beta_deg};
-                sc.fitted[f] = 1;
+                line[f] = ps_line{24 * b.per, b.dev, b.dev * b.dev * obj.n_points,
+                                  f == 0 ? conw_r * obj.escl * obj.escl : b.dark, b.lambda_deg, b.beta_deg};
+                rms[q] = b.dev;
             }
             return true;
         };
-        // fits the unfitted frequencies among [lo, hi] whose mask is set
-        auto fit = [&](int lo, int hi, const std::vector<char> *mask) {
-            std::vector<int> sel;
-            for (int f = std::max(0, lo); f <= std::min(n_last - 1, hi); ++f)
-                if (!sc.fitted[f] && (!mask || (*mask)[f])) sel.push_back(f);
-            return fit_list(sel);
-        };
-        std::vector<char> first(n_last);
-        for (int f = 0; f < n_last; ++f) first[f] = core[f] || aud[f];
-        bool ok = fit(0, n_last - 1, &first);
-        for (int f = 0; f < n_last; ++f) sc.initial += sc.fitted[f];
-        std::vector<char> probed(n_last, 0);
-        while (ok && !sc.fallback) {
-            // widen around a best line at the edge of a fitted run
-            while (ok) {
-                const int b = best_fitted(sc);
-                if (b < 0) {
-                    sc.fallback = true;
-                    sc.reason = "edge";
-                    break;
-                }
-                const bool open = (b > 0 && !sc.fitted[b - 1]) || (b + 1 < n_last && !sc.fitted[b + 1]);
-                if (!open) break;
-                if (sc.expansions >= kMaxExpansions) {
-                    sc.fallback = true;
-                    sc.reason = "edge";
-                    break;
-                }
-                ok = fit(b - kEdge, b + kEdge, nullptr);
-                ++sc.expansions;
-            }
-            if (!ok || sc.fallback) break;
-            // probe the best line's period-doubling partners (twice and half its frequency) once
-            const int b = best_fitted(sc);
-            if (probed[b]) break;
-            probed[b] = 1;
-            for (int a : alias_indices(obj.freq_start, obj.freq_step, n_last, b))
-                if (ok) ok = fit(a - kEdge, a + kEdge, nullptr);
-            ++sc.alias_probes;
-            if (best_fitted(sc) == b) break;
-        }
-        if (ok && !sc.fallback) {
-            const int b = best_fitted(sc);
-            for (int a = 0; a < n_last; ++a)
-                if (aud[a] && std::abs(a - b) > kEdge && sc.line[a].rms <= sc.line[b].rms * (1.0 + kAuditMargin)) {
-                    sc.fallback = true;
-                    sc.reason = "audit";
-                    break;
-                }
-        }
-        if (ok && sc.fallback) ok = fit(0, n_last - 1, nullptr);
+        bool ok = psflow::run_plan(sc, core, aud, obj.freq_start, obj.freq_step, fit);
         if (ok && opt.precision == PS_PRECISION_MIXED) {
             // the candidates' final fits in FP64
             ok = ps_gpu_set_precision(h, PS_PRECISION_FP64) == PS_OK &&
                  ps_gpu_configure(h, obj.freq_start, obj.freq_step, obj.stop_condition, obj.n_iter_min, conw_r,
                                   conw_r, obj.n_points, obj.ia.data(), ia_par, obj.cg_first.data(), obj.sig.data(),
-                                  obj.sigr2.data(), obj.n_fac, obj.brightness.data(), &curves, &shape) == PS_OK;
-            std::vector<char> done(n_last, 0);
-            for (int round = 0; ok && round < kPolishRounds; ++round) {
-                const int b = best_fitted(sc);
-                if (b < 0) break;
-                const std::vector<int> sel = polish_set(sc, obj.freq_start, obj.freq_step, b, round == 0, done);
-                if (sel.empty()) break;
-                ok = fit_list(sel);
-                for (int f : sel) done[f] = 1;
-                sc.polished += (int)sel.size();
-            }
+                                  obj.sigr2.data(), obj.n_fac, obj.brightness.data(), &curves, &shape) == PS_OK &&
+                 psflow::polish(sc, obj.freq_start, obj.freq_step, fit);
         }
         if (!ok) {
             std::fclose(out);
@@ -524,7 +349,7 @@ int main(int argc, char **argv)
         int n_fit = 0;
         for (int f = 0; f < n_last; ++f)
             if (sc.fitted[f]) {
-                print_line(out, sc.line[f]);
+                print_line(out, line[f]);
                 ++n_fit;
             }
         std::fclose(out);
