@@ -664,7 +664,8 @@ def main():
               "first_selection": plan.initial, "edge_expansions": plan.expansions,
               "period_doubling_probes": plan.alias_probes, "fallback": plan.fallback,
               "fallback_reason": plan.reason, "n_frequencies": int(n_max),
-              "fits": int(10 * (len(idx) + plan.polished)), "fp64_refitted_frequencies": plan.polished,
+              "fits": int(10 * (plan.first_pass + plan.polished)), "mixed_fitted_frequencies": plan.first_pass,
+              "fp64_refitted_frequencies": plan.polished,
               "vs_plain_fp64_full_scan_s": n_max * 10 / value,
               "speedup_vs_plain_fp64_full_scan": (n_max * 10 / value) / screened_s,
               "best_frequency": int(idx[b]),

@@ -253,6 +253,7 @@ class Plan:
         self.alias_probes = 0    # best lines whose period-doubling partners were fitted
         self.fallback = False    # the whole grid was fitted
         self.reason = ""         # why it fell back: "audit" or "edge"
+        self.first_pass = 0      # frequencies fitted before any FP64 refit
         self.polished = 0        # mixed precision: frequencies refitted in FP64
         self.polish_rounds = 0
 
@@ -447,6 +448,7 @@ def screened_scan(obj, net, conw_r, top=0.034, halo=1, audit=0.02, seed=0, devic
             return lines[:, 1]
 
         plan = plan_scan(pred, fit, top, halo, audit, seed, margin, freqs=frequencies(obj))
+        plan.first_pass = len(plan.rms)
         if precision == native.PRECISION_MIXED and polish:
             # the candidates' final fits in FP64 (polish_plan)
             eng.set_precision(native.PRECISION_FP64)
